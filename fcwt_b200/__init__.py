@@ -1,0 +1,14 @@
+"""fcwt_b200 — B200-native (sm_100a) fast continuous wavelet transform.
+
+Drop-in for the transform path of fastlib/fCWT: ``import fcwt_b200 as fcwt``
+gives the reference module's names (Morlet, Scales, FCWT with cwt/ccwt,
+create_FFT_optimization_plan, the FCWT_* scale types and the ``cwt``
+boilerplate). The transform runs in hand-written CUDA kernels behind the C ABI
+of lib/libfcwt_b200.so; there is no CPU fallback.
+"""
+from ._lib import FcwtError, FCWT_OUT_BF16, FCWT_OUT_C64, FCWT_OUT_F16, LIB_PATH  # noqa: F401
+from .api import (FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, Morlet, Plan, Scales,  # noqa: F401
+                  Wavelet, cwt, cwt_device, mother_host, row_truncation, synchronize)
+
+__all__ = ["Morlet", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
+           "cwt_device", "Plan", "synchronize", "row_truncation", "mother_host", "FcwtError"]

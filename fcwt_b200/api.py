@@ -1,0 +1,437 @@
+"""Python mirror of the reference's fcwt module (src/fcwt/fcwt.i, fcwt.py,
+boilerplate.py of fastlib/fCWT) over the C ABI of libfcwt_b200.so.
+
+Same names, arguments, in-place output conventions and errors as the SWIG
+module, so code and tests written for ``import fcwt`` run against
+``import fcwt_b200 as fcwt``. Inputs and outputs may be numpy arrays (host) or
+torch CUDA tensors (device-resident; nothing is copied, work is enqueued on
+torch's current stream). torch is imported only when a tensor is passed.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+from . import _lib
+from ._lib import (FCWT_EXACT_SUPPORT, FCWT_NORM, FCWT_OUT_BF16, FCWT_OUT_C64, FCWT_OUT_F16,
+                   FCWT_SCALAR_TRUNC, FcwtError)
+
+# enum SCALETYPE (src/fcwt/fcwt.h:65)
+FCWT_LINSCALES = 0
+FCWT_LOGSCALES = 1
+FCWT_LINFREQS = 2
+
+_FFTW_FLAGS = {"FFTW_MEASURE": 1, "FFTW_PATIENT": 2, "FFTW_EXHAUSTIVE": 3, "FFTW_ESTIMATE": 0}
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _positive(name: str, v) -> None:
+    # fcwt.i:28-32: %typemap(check) float f0, float f1, int fn
+    if v <= 0:
+        raise ValueError("Expected a non-zero, positive value.")
+
+
+def _as_int(name: str, v) -> int:
+    if isinstance(v, (bool, np.bool_)):
+        raise TypeError(f"argument '{name}' must be an int")
+    if isinstance(v, (int, np.integer)):
+        return int(v)
+    if isinstance(v, (float, np.floating)) and float(v).is_integer():
+        return int(v)
+    raise TypeError(f"argument '{name}' must be an int")
+
+
+class Wavelet:
+    """Base class of the reference's wavelet interface (src/fcwt/fcwt.h:67-79)."""
+
+    def __init__(self):
+        self.width = 0
+        self.four_wavelen = 0.0
+        self.imag_frequency = False
+        self.doublesided = False
+        self.mother = None
+
+    def generate(self, *args):
+        raise NotImplementedError("Override this virtual class")
+
+    def getSupport(self, scale):
+        raise NotImplementedError("Override this virtual class")
+
+    def getWavelet(self, scale, pwav):
+        raise NotImplementedError("Override this virtual class")
+
+
+class Morlet(Wavelet):
+    """Morlet(bandwidth) (src/fcwt/fcwt.cpp:41-49)."""
+
+    def __init__(self, bandwidth):
+        super().__init__()
+        self.fb = float(np.float32(bandwidth))
+        self.four_wavelen = float(np.float32(0.9876))
+
+    def generate(self, *args):
+        """generate(size): frequency-domain mother table of length size, computed
+        on the GPU (src/fcwt/fcwt.cpp:51-67); stored in ``self.mother``.
+        generate(real, imag, size, scale): time-domain wavelet written into the
+        float32 arrays real/imag (2*getSupport(scale)+1 taps, fcwt.cpp:68-84)."""
+        if len(args) == 1:
+            size = _as_int("size", args[0])
+            self.width = size
+            out = np.zeros(max(size, 0), np.float32)
+            if size > 0:
+                _lib.call("fcwt_morlet_mother", _lib.context().handle, ctypes.c_float(self.fb), size, _ptr(out))
+            self.mother = out
+            return None
+        if len(args) == 4:
+            real, imag, size, scale = args
+            w = self.getSupport(scale)
+            for a in (real, imag):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+                    raise TypeError("real/imag must be contiguous float32 arrays")
+                if a.size < 2 * w + 1:
+                    raise ValueError("real/imag must hold 2*getSupport(scale)+1 values")
+            self.width = w
+            _lib.call("fcwt_morlet_time", ctypes.c_float(self.fb), ctypes.c_float(scale), _as_int("size", size),
+                      _ptr(real), _ptr(imag))
+            return None
+        raise TypeError("generate() takes (size) or (real, imag, size, scale)")
+
+    def getSupport(self, scale) -> int:
+        return _lib.load().fcwt_morlet_support(ctypes.c_float(self.fb), ctypes.c_float(scale))
+
+    def getWavelet(self, scale, pwav) -> None:
+        """Fill the complex64 array pwav in place (src/fcwt/fcwt.cpp:86-105)."""
+        if not (isinstance(pwav, np.ndarray) and pwav.dtype == np.complex64 and pwav.flags.c_contiguous
+                and pwav.ndim == 1):
+            raise TypeError("pwav must be a contiguous 1-D complex64 array")
+        _lib.call("fcwt_morlet_wavelet", ctypes.c_float(self.fb), ctypes.c_float(scale), _ptr(pwav), pwav.size)
+
+
+class Scales:
+    """Scales(wavelet, scaletype, fs, f0, f1, fn) (src/fcwt/fcwt.cpp:111-190)."""
+
+    def __init__(self, pwav, st, fs, f0, f1, fn):
+        fs = _as_int("fs", fs)
+        fn = _as_int("fn", fn)
+        _positive("f0", f0)
+        _positive("f1", f1)
+        _positive("fn", fn)
+        st = _as_int("st", st)
+        self.fs = fs
+        self.fourwavl = float(getattr(pwav, "four_wavelen", np.float32(0.9876)))
+        self.nscales = fn
+        self.scales = np.zeros(fn, np.float32)
+        _lib.call("fcwt_scales", st, fs, ctypes.c_float(f0), ctypes.c_float(f1), fn, _ptr(self.scales))
+
+    def getScales(self, pfreqs) -> None:
+        pfreqs = _inplace_f32(pfreqs)
+        n = min(pfreqs.size, self.scales.size)
+        pfreqs[:n] = self.scales[:n]
+
+    def getFrequencies(self, pfreqs) -> None:
+        pfreqs = _inplace_f32(pfreqs)
+        n = pfreqs.size
+        if n > self.scales.size:
+            raise ValueError("array longer than the number of scales")
+        _lib.call("fcwt_frequencies", _ptr(self.scales), n, self.fs, _ptr(pfreqs))
+
+
+def _inplace_f32(a) -> np.ndarray:
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous and a.ndim == 1):
+        raise TypeError("Array of type 'float' required (contiguous, 1-D)")
+    return a
+
+
+def _scales_array(scales) -> np.ndarray:
+    if isinstance(scales, Scales):
+        return scales.scales
+    return np.ascontiguousarray(scales, np.float32)
+
+
+class FCWT:
+    """FCWT(wavelet, threads, use_optimalization_schemes, use_normalization)
+    (src/fcwt/fcwt.h:114-152). ``threads`` keeps its reference meaning for
+    the result: it sets the per-scale truncation length (fcwt.cpp:213-214)."""
+
+    def __init__(self, pwav, pthreads, puse_optimalization_schemes, puse_normalization, device: int = 0):
+        self.wavelet = pwav
+        self.threads = _as_int("pthreads", pthreads)
+        self.use_optimalization_schemes = bool(puse_optimalization_schemes)
+        self.use_normalization = bool(puse_normalization)
+        self.device = device
+        self.flags = FCWT_NORM if self.use_normalization else 0
+
+    # -- tuning files (src/fcwt/fcwt.cpp:313-393)
+    def create_FFT_optimization_plan(self, pmaxsize, poptimizationflags) -> None:
+        if isinstance(poptimizationflags, str):
+            if poptimizationflags not in _FFTW_FLAGS:
+                print(f"Unknown flag: {poptimizationflags}", file=sys.stderr)
+                return
+            level = _FFTW_FLAGS[poptimizationflags]
+        else:
+            f = _as_int("poptimizationflags", poptimizationflags)
+            # FFTW flag bits: ESTIMATE 1<<6, EXHAUSTIVE 1<<3, PATIENT 1<<5, MEASURE 0
+            level = 0 if f & (1 << 6) else 3 if f & (1 << 3) else 2 if f & (1 << 5) else 1
+        pmaxsize = _as_int("pmaxsize", pmaxsize)
+        if _lib.load().fcwt_find2power(pmaxsize) <= 10:
+            print("Maxsize is too small (<=1024)... please use a larger number", file=sys.stderr)
+        _lib.call("fcwt_create_optimization_plan", _lib.context(self.device).handle, pmaxsize, self.threads,
+                  level, None)
+
+    def _load_plan(self, n: int) -> None:
+        if not self.use_optimalization_schemes:
+            return
+        N = 1 << _lib.load().fcwt_find2power(n)
+        if N <= 1024:
+            print("Inputsize is too small (N <= 1024) to use optimization.")
+            return
+        rc = _lib.load().fcwt_load_optimization_plan(_lib.context(self.device).handle, n, self.threads, None)
+        if rc != 0:
+            print(f"WARNING: Optimization scheme 'n{N}_t{self.threads}.wis' was not found, "
+                  "fallback to calculation without optimization.")
+
+    def cwt(self, pinput, scales, poutput, out_type: int = FCWT_OUT_C64) -> None:
+        """FCWT::cwt(input, n, scales, output, n1, n2) (fcwt.cpp:540-543):
+        real input; output [fn, n] complex64 written in place."""
+        self._run(pinput, scales, poutput, False, out_type)
+
+    def ccwt(self, pcinput, scales, poutput, out_type: int = FCWT_OUT_C64) -> None:
+        """FCWT::cwt(complex input, ...) (fcwt.cpp:545-548)."""
+        self._run(pcinput, scales, poutput, True, out_type)
+
+    def _run(self, x, scales, out, complex_input: bool, out_type: int) -> None:
+        sc = _scales_array(scales)
+        if not isinstance(self.wavelet, Morlet):
+            raise TypeError("only the Morlet wavelet has a GPU transform")
+        fb = self.wavelet.fb
+        ctx = _lib.context(self.device)
+        fname = "fcwt_ccwt" if complex_input else "fcwt_cwt"
+        if _is_torch(x) or _is_torch(out):
+            _run_torch(ctx, fname, x, sc, out, complex_input, fb, self.threads, self.flags, out_type)
+            return
+        xin = _host_input(x, complex_input)
+        n = xin.size
+        self._load_plan(n)
+        _check_host_output(out, sc.size, n, out_type)
+        _lib.call(fname, ctx.handle, _ptr(xin), n, ctypes.c_float(fb), _ptr(sc), sc.size, self.threads,
+                  self.flags, _ptr(out), out_type)
+
+
+def _host_input(x, complex_input: bool) -> np.ndarray:
+    x = np.asarray(x)
+    if x.ndim != 1:
+        raise ValueError("Array must be 1-dimensional")
+    if complex_input:
+        if not np.iscomplexobj(x) and x.dtype.kind not in "fiu":
+            raise TypeError("Array of type 'complex float' required")
+        return np.ascontiguousarray(x, np.complex64)
+    if np.iscomplexobj(x):
+        raise TypeError("Array of type 'float' required")
+    return np.ascontiguousarray(x, np.float32)
+
+
+_OUT_DTYPES = {FCWT_OUT_C64: (np.complex64,), FCWT_OUT_BF16: (np.uint32, np.float32), FCWT_OUT_F16: (np.uint32, np.float32)}
+
+
+def _check_host_output(out, fn: int, n: int, out_type: int) -> None:
+    if not isinstance(out, np.ndarray):
+        raise TypeError("output must be a numpy array or a torch CUDA tensor")
+    if not out.flags.c_contiguous:
+        raise TypeError("Array must be contiguous.")
+    if out_type == FCWT_OUT_C64:
+        if out.dtype != np.complex64:
+            raise TypeError("Array of type 'complex float' required")
+        if out.size != fn * n:
+            raise ValueError(f"output must hold nscales*n = {fn}*{n} values")
+    else:
+        if out.nbytes != fn * n * 4:
+            raise ValueError(f"output must hold nscales*n*4 bytes for a 16-bit complex type")
+
+
+def _run_torch(ctx, fname, x, sc, out, complex_input, fb, threads, flags, out_type) -> None:
+    import torch
+
+    if not (isinstance(x, torch.Tensor) and isinstance(out, torch.Tensor)):
+        raise TypeError("pass both input and output as torch tensors for the device path")
+    if not (x.is_cuda and out.is_cuda):
+        raise TypeError("torch tensors must live on a CUDA device")
+    if x.dim() != 1:
+        raise ValueError("Array must be 1-dimensional")
+    want = torch.complex64 if complex_input else torch.float32
+    if x.dtype != want:
+        raise TypeError(f"input must be {want}")
+    if not x.is_contiguous() or not out.is_contiguous():
+        raise TypeError("tensors must be contiguous")
+    n = x.numel()
+    esz = 8 if out_type == FCWT_OUT_C64 else 4
+    if out.numel() * out.element_size() != sc.size * n * esz:
+        raise ValueError("output has the wrong size")
+    if out.device.index != ctx.device:
+        ctx = _lib.context(out.device.index)
+    ctx.set_stream(torch.cuda.current_stream(out.device).cuda_stream)
+    try:
+        _lib.call(fname, ctx.handle, ctypes.c_void_p(x.data_ptr()), n, ctypes.c_float(fb), _ptr(sc), sc.size,
+                  threads, flags, ctypes.c_void_p(out.data_ptr()), out_type)
+    finally:
+        ctx.set_stream(None)
+
+
+class Plan:
+    """A reusable device plan (fcwt_plan_create): all shape-, scale- and
+    flag-dependent work done once; ``execute`` runs one transform.
+
+    rows=(begin, end) selects a shard of the scale rows (multi-GPU sharding);
+    the reference's stale-bin semantics still follow all rows."""
+
+    def __init__(self, n: int, scales, fb: float = 2.0, threads: int = 1, norm: bool = True,
+                 complex_input: bool = False, rows: tuple[int, int] | None = None, device: int = 0,
+                 exact_support: bool = False, scalar_trunc: bool = False):
+        self.ctx = _lib.context(device)
+        self.device = device
+        self.scales = _scales_array(scales).copy()
+        self.n = int(n)
+        self.fn = self.scales.size
+        self.rows = rows if rows is not None else (0, self.fn)
+        self.complex_input = complex_input
+        flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0) | \
+            (FCWT_SCALAR_TRUNC if scalar_trunc else 0)
+        h = ctypes.c_void_p()
+        _lib.call("fcwt_plan_create", self.ctx.handle, self.n, 1 if complex_input else 0, ctypes.c_float(fb),
+                  _ptr(self.scales), self.fn, int(threads), flags, int(self.rows[0]), int(self.rows[1]),
+                  ctypes.byref(h))
+        self.handle = h
+
+    @property
+    def n_rows(self) -> int:
+        return self.rows[1] - self.rows[0]
+
+    def execute(self, x, out, out_type: int = FCWT_OUT_C64, stream=None) -> None:
+        """x, out: numpy arrays (host; synchronous) or torch CUDA tensors (enqueued
+        on `stream` or torch's current stream)."""
+        if _is_torch(x) or _is_torch(out):
+            import torch
+
+            st = stream if stream is not None else torch.cuda.current_stream(self.device)
+            self.ctx.set_stream(st.cuda_stream)
+            try:
+                _lib.call("fcwt_plan_execute", self.handle, ctypes.c_void_p(x.data_ptr()),
+                          ctypes.c_void_p(out.data_ptr()), out_type)
+            finally:
+                self.ctx.set_stream(None)
+            return
+        xin = _host_input(x, self.complex_input)
+        if xin.size != self.n:
+            raise ValueError("input length differs from the plan")
+        _check_host_output(out, self.n_rows, self.n, out_type)
+        _lib.call("fcwt_plan_execute", self.handle, _ptr(xin), _ptr(out), out_type)
+
+    def execute_ptr(self, x_ptr: int, out_ptr: int, out_type: int = FCWT_OUT_C64, stream_ptr: int = 0) -> None:
+        """Raw-pointer form (device or host pointers)."""
+        self.ctx.set_stream(stream_ptr)
+        try:
+            _lib.call("fcwt_plan_execute", self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(out_ptr), out_type)
+        finally:
+            self.ctx.set_stream(None)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().fcwt_plan_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def synchronize(device: int = 0) -> None:
+    """Wait for the device work of this process's context and raise on device errors."""
+    _lib.context(device).synchronize()
+
+
+def row_truncation(n: int, scales, threads: int = 1, exact_support: bool = False, scalar_trunc: bool = False,
+                   fb: float = 2.0):
+    """Per-row truncation length of the reference (bit-exact) and the bin window
+    [lo, hi) the device engine evaluates for Morlet(fb). Host only."""
+    sc = _scales_array(scales)
+    proc = np.zeros(sc.size, np.int32)
+    lo = np.zeros(sc.size, np.int32)
+    hi = np.zeros(sc.size, np.int32)
+    flags = (FCWT_EXACT_SUPPORT if exact_support else 0) | (FCWT_SCALAR_TRUNC if scalar_trunc else 0)
+    _lib.call("fcwt_row_truncation", int(n), ctypes.c_float(fb), _ptr(sc), sc.size, int(threads), flags, _ptr(proc),
+              _ptr(lo), _ptr(hi))
+    return proc, lo, hi
+
+
+def mother_host(fb: float, N: int) -> np.ndarray:
+    """Morlet::generate(int) evaluated by the library's host code (no GPU)."""
+    out = np.zeros(N, np.float32)
+    _lib.call("fcwt_morlet_mother_host", ctypes.c_float(fb), int(N), _ptr(out))
+    return out
+
+
+# ---------------------------------------------------------------- boilerplate
+
+def cwt(input, fs, f0, f1, fn, nthreads=1, scaling="lin", fast=False, norm=True):
+    """fcwt.cwt (src/fcwt/boilerplate.py:5-33): Morlet(2.0), LINFREQS for
+    scaling="lin" else LOGSCALES; returns (freqs float32[fn], out complex64[fn, n])."""
+    if _is_torch(input):
+        return cwt_device(input, fs, f0, f1, fn, nthreads=nthreads, scaling=scaling, norm=norm)
+    input = np.asarray(input)
+    if input.ndim > 1:
+        raise ValueError("Input must be a vector")
+    if input.dtype != np.float32:
+        input = input.astype(np.float32)
+    morl = Morlet(2.0)
+    if scaling == "lin":
+        scales = Scales(morl, FCWT_LINFREQS, fs, f0, f1, fn)
+    else:
+        scales = Scales(morl, FCWT_LOGSCALES, fs, f0, f1, fn)
+    fcwt = FCWT(morl, nthreads, fast, norm)
+    output = np.zeros((fn, input.size), dtype=np.complex64)
+    freqs = np.zeros((fn), dtype=np.float32)
+    fcwt.cwt(input, scales, output)
+    scales.getFrequencies(freqs)
+    return freqs, output
+
+
+def cwt_device(input, fs, f0, f1, fn, nthreads=1, scaling="lin", norm=True, out_dtype=None, fb: float = 2.0):
+    """Device-resident form of fcwt.cwt for a torch CUDA tensor: returns
+    (freqs numpy float32[fn], out torch tensor [fn, n]) without host copies.
+    out_dtype: torch.complex64 (default) or torch.bfloat16 / torch.float16 for
+    interleaved 16-bit (re, im) pairs, shape [fn, n, 2]."""
+    import torch
+
+    x = input
+    if x.dim() != 1:
+        raise ValueError("Input must be a vector")
+    if x.dtype != torch.float32:
+        x = x.float()
+    x = x.contiguous()
+    morl = Morlet(fb)
+    st = FCWT_LINFREQS if scaling == "lin" else FCWT_LOGSCALES
+    scales = Scales(morl, st, fs, f0, f1, fn)
+    n = x.numel()
+    if out_dtype is None or out_dtype == torch.complex64:
+        out = torch.empty((fn, n), dtype=torch.complex64, device=x.device)
+        ot = FCWT_OUT_C64
+    elif out_dtype in (torch.bfloat16, torch.float16):
+        out = torch.empty((fn, n, 2), dtype=out_dtype, device=x.device)
+        ot = FCWT_OUT_BF16 if out_dtype == torch.bfloat16 else FCWT_OUT_F16
+    else:
+        raise TypeError("out_dtype must be complex64, bfloat16 or float16")
+    FCWT(morl, nthreads, False, norm, device=x.device.index or 0).cwt(x, scales, out, out_type=ot)
+    freqs = np.zeros(fn, np.float32)
+    scales.getFrequencies(freqs)
+    return freqs, out

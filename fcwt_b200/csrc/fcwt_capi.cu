@@ -1,0 +1,744 @@
+// C ABI of the B200 fCWT path: contexts, plans, transforms and tuning files.
+// See include/fcwt_b200.h for the contract of each entry point.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/fcwt_b200.h"
+#include "fcwt_internal.h"
+#include "fcwt_plan.h"
+
+namespace fcwt {
+size_t engine_smem_bytes();
+cudaError_t launch_mother(float fb, int N, float norm, float* out, cudaStream_t st);
+cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st);
+cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
+                           float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
+cudaError_t engine_configure();
+cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
+}  // namespace fcwt
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define FCWT_CUDA_TRY(expr)                                                                  \
+    do {                                                                                     \
+        cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? FCWT_ERR_NOMEM : FCWT_ERR_CUDA,    \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                \
+        }                                                                                    \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            bytes = 0;
+            return e;
+        }
+        bytes = b;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+// Scheduling choices of the two-phase row engine for one padded length.
+struct TuneChoice {
+    int scratch_mb = 64;  // budget of the scratch ring
+    int lag = 12;         // rows between a row's phase 1 and phase 2 items
+};
+
+bool is_device_pointer(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+size_t out_elem_bytes(int out_type) { return out_type == FCWT_OUT_C64 ? 8 : 4; }
+
+}  // namespace
+
+struct fcwt_plan;
+
+struct fcwt_context {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    DevBuf in_stage, out_stage, tmp, scratch, counters, err;
+    int* err_host = nullptr;  // pinned mirror of the device error word
+    TuneChoice tune[fcwt::kMaxLog2N + 1];
+    struct CacheEntry {
+        int n, is_complex, fn, threads;
+        unsigned flags;
+        float fb;
+        std::vector<float> scales;
+        fcwt_plan* plan;
+        unsigned long long last_use;
+    };
+    std::vector<CacheEntry> cache;
+    unsigned long long use_clock = 0;
+    // profiling
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;
+    long long kernel_launches = 0;
+};
+
+struct fcwt_plan {
+    fcwt_context* ctx = nullptr;
+    fcwt::SignalPlan sp;
+    int rb = 0, re = 0;
+    DevBuf X, mother, tw, pool, sigs, rows, items;
+    int n_items = 0;
+    int n_rows = 0;
+    int slots = 0;
+    long long slot_elems = 0;
+    bool two_phase = false;
+};
+
+namespace {
+
+int ctx_prepare(fcwt_context* ctx) {
+    if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
+    FCWT_CUDA_TRY(cudaSetDevice(ctx->device));
+    return FCWT_OK;
+}
+
+void plan_free(fcwt_plan* p) {
+    if (!p) return;
+    p->X.release();
+    p->mother.release();
+    p->tw.release();
+    p->pool.release();
+    p->sigs.release();
+    p->rows.release();
+    p->items.release();
+    delete p;
+}
+
+// Builds the work list: small / fused rows get one item each; two-phase rows
+// get n_a phase-1 items and n_b phase-2 items, phase 2 of row r issued after
+// phase 1 of row r + lag, scratch slots reused round-robin.
+int plan_build(fcwt_plan* P) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    const SignalPlan& sp = P->sp;
+    const int N = sp.N;
+    const int M = sp.M;
+    P->n_rows = P->re - P->rb;
+    std::vector<RowDesc> rows((size_t)P->n_rows);
+    std::vector<Item> items;
+    // stale pool: concatenated tables
+    std::vector<float> pool;
+    pool.reserve(sp.tables.size() * (size_t)sp.half);
+    for (const auto& T : sp.tables) pool.insert(pool.end(), T.begin(), T.end());
+    const float out_scale = (sp.flags & kFlagNorm) ? 1.0f / (float)N : 1.0f;
+    for (int r = 0; r < P->n_rows; r++) {
+        const RowPlan& rp = sp.rows[(size_t)(P->rb + r)];
+        RowDesc& d = rows[(size_t)r];
+        d.sig = 0;
+        d.proc = rp.proc;
+        d.step = rp.step;
+        d.K = rp.K;
+        d.L = rp.L;
+        d.lo = rp.lo;
+        d.hi = rp.hi;
+        d.stale = rp.table >= 0 ? rp.table * sp.half : -1;
+        d.slot = -1;
+        d.wait_row = -1;
+        d.n_a = 0;
+        d.n_b = 0;
+        d.out_buf = 0;
+        d.out_off = (long long)r * sp.n;
+        d.out_scale = out_scale;
+        d.pad = 0;
+        if (N >= kP2 && rp.K > kMaxK)
+            return fail(FCWT_ERR_UNSUPPORTED,
+                        "row support wider than 32768 bins at N > 16384 is not implemented in this build");
+    }
+    P->two_phase = N > kMaxFusedN;
+    if (!P->two_phase) {
+        const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;
+        for (int r = 0; r < P->n_rows; r++) items.push_back({type, r, 0, 0});
+        P->slots = 0;
+        P->slot_elems = 0;
+    } else {
+        const TuneChoice& tc = ctx->tune[sp.log2N];
+        const long long slot_bytes = (long long)N * 8;
+        int S = (int)std::max(4LL, std::min(40LL, ((long long)tc.scratch_mb << 20) / slot_bytes));
+        S = std::min(S, std::max(1, P->n_rows));
+        int D = std::max(1, std::min(tc.lag, S / 2));
+        if (S == 1) D = 1;
+        const int n_a = kP2 / kChunk;
+        const int n_b = M / kGroupCols;
+        for (int r = 0; r < P->n_rows; r++) {
+            rows[(size_t)r].slot = r % S;
+            rows[(size_t)r].wait_row = r >= S ? r - S : -1;
+            rows[(size_t)r].n_a = n_a;
+            rows[(size_t)r].n_b = n_b;
+        }
+        for (int step = 0; step < P->n_rows + D; step++) {
+            if (step < P->n_rows)
+                for (int a = 0; a < n_a; a++) items.push_back({ITEM_PHASE1, step, a, 0});
+            const int rb = step - D;
+            if (rb >= 0 && rb < P->n_rows)
+                for (int b = 0; b < n_b; b++) items.push_back({ITEM_PHASE2, rb, b, 0});
+        }
+        P->slots = S;
+        P->slot_elems = N;
+        // the lag must not exceed the slot count (phase 1 of row r waits on
+        // phase 2 of row r - S, which must already be issued)
+        if (D >= S && S > 1) return fail(FCWT_ERR_INVALID, "internal: lag >= slots");
+    }
+    P->n_items = (int)items.size();
+
+    cudaStream_t st = ctx->stream;
+    FCWT_CUDA_TRY(P->X.ensure((size_t)N * sizeof(float2)));
+    FCWT_CUDA_TRY(P->mother.ensure((size_t)N * sizeof(float)));
+    const int tw_n = 1024 + std::max(M, 1);
+    FCWT_CUDA_TRY(P->tw.ensure((size_t)tw_n * sizeof(float2)));
+    FCWT_CUDA_TRY(P->pool.ensure(std::max<size_t>(pool.size(), 1) * sizeof(float)));
+    FCWT_CUDA_TRY(P->sigs.ensure(sizeof(SigDesc)));
+    FCWT_CUDA_TRY(P->rows.ensure(std::max<size_t>(rows.size(), 1) * sizeof(RowDesc)));
+    FCWT_CUDA_TRY(P->items.ensure(std::max<size_t>(items.size(), 1) * sizeof(Item)));
+    FCWT_CUDA_TRY(launch_mother(sp.fb, N, host::mother_norm(), P->mother.as<float>(), st));
+    FCWT_CUDA_TRY(launch_twiddle(sp.log2N, P->tw.as<float2>(), st));
+    SigDesc sd;
+    sd.X = P->X.as<float2>();
+    sd.mother = P->mother.as<float>();
+    sd.tw = P->tw.as<float2>();
+    sd.log2N = sp.log2N;
+    sd.n = sp.n;
+    if (!pool.empty())
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->pool.p, pool.data(), pool.size() * sizeof(float),
+                                      cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(cudaMemcpyAsync(P->sigs.p, &sd, sizeof(sd), cudaMemcpyHostToDevice, st));
+    if (!rows.empty())
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->rows.p, rows.data(), rows.size() * sizeof(RowDesc),
+                                      cudaMemcpyHostToDevice, st));
+    if (!items.empty())
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->items.p, items.data(), items.size() * sizeof(Item),
+                                      cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+    return FCWT_OK;
+}
+
+int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
+        return fail(FCWT_ERR_INVALID, "unknown output type");
+    const SignalPlan& sp = P->sp;
+    const int n = sp.n;
+    if (n == 0 || P->n_rows == 0) return FCWT_OK;
+    if (!input || !output) return fail(FCWT_ERR_INVALID, "null input or output pointer");
+    cudaStream_t st = ctx->stream;
+    const size_t in_bytes = (size_t)n * (sp.is_complex ? 8 : 4);
+    const size_t out_bytes = (size_t)P->n_rows * (size_t)n * out_elem_bytes(out_type);
+    const void* din = input;
+    if (!is_device_pointer(input)) {
+        FCWT_CUDA_TRY(ctx->in_stage.ensure(in_bytes));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->in_stage.p, input, in_bytes, cudaMemcpyHostToDevice, st));
+        din = ctx->in_stage.p;
+    }
+    const bool host_out = !is_device_pointer(output);
+    void* dout = output;
+    if (host_out) {
+        FCWT_CUDA_TRY(ctx->out_stage.ensure(out_bytes));
+        dout = ctx->out_stage.p;
+    }
+    FCWT_CUDA_TRY(ctx->tmp.ensure((size_t)sp.N * sizeof(float2)));
+    int n_fwd = 0;
+    FCWT_CUDA_TRY(launch_forward(sp.is_complex ? nullptr : (const float*)din,
+                                 sp.is_complex ? (const float2*)din : nullptr, n, sp.log2N,
+                                 P->tw.as<float2>(), P->X.as<float2>(), ctx->tmp.as<float2>(), st, &n_fwd));
+    ctx->kernel_launches += n_fwd;
+    const size_t n_counters = 1 + 2 * (size_t)P->n_rows;
+    FCWT_CUDA_TRY(ctx->counters.ensure(n_counters * sizeof(unsigned)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, n_counters * sizeof(unsigned), st));
+    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
+    if (P->two_phase)
+        FCWT_CUDA_TRY(ctx->scratch.ensure((size_t)P->slots * (size_t)P->slot_elems * sizeof(float2)));
+    EngineParams ep;
+    std::memset(&ep, 0, sizeof(ep));
+    ep.sigs = P->sigs.as<SigDesc>();
+    ep.rows = P->rows.as<RowDesc>();
+    ep.items = P->items.as<Item>();
+    ep.n_items = P->n_items;
+    ep.stale_pool = P->pool.as<float>();
+    ep.scratch = P->two_phase ? ctx->scratch.as<float2>() : nullptr;
+    ep.slot_elems = P->slot_elems;
+    ep.counters = ctx->counters.as<unsigned>();
+    ep.n_rows = P->n_rows;
+    ep.outs[0] = dout;
+    ep.out_type = out_type;
+    ep.err = ctx->err.as<int>();
+    const int grid = std::max(1, std::min(P->n_items, ctx->num_sms));
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    if (ctx->profiling) {
+        if (!ctx->ev_free.empty()) {
+            ev = ctx->ev_free.back();
+            ctx->ev_free.pop_back();
+        } else {
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
+        }
+        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
+    }
+    FCWT_CUDA_TRY(launch_engine(ep, grid, st));
+    ctx->kernel_launches += 1;
+    if (ctx->profiling) {
+        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
+        ctx->ev_used.push_back(ev);
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (host_out) {
+        FCWT_CUDA_TRY(cudaMemcpyAsync(output, dout, out_bytes, cudaMemcpyDeviceToHost, st));
+        FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+        if (*ctx->err_host != 0)
+            return fail(FCWT_ERR_DEVICE, "row engine reported error bits " + std::to_string(*ctx->err_host));
+    }
+    return FCWT_OK;
+}
+
+bool key_match(const fcwt_context::CacheEntry& e, int n, int cplx, float fb, const float* scales, int fn,
+               int threads, unsigned flags) {
+    return e.n == n && e.is_complex == cplx && e.fb == fb && e.fn == fn && e.threads == threads &&
+           e.flags == flags && std::memcmp(e.scales.data(), scales, sizeof(float) * (size_t)fn) == 0;
+}
+
+int cached_plan(fcwt_context* ctx, int n, int cplx, float fb, const float* scales, int fn, int threads,
+                unsigned flags, fcwt_plan** out) {
+    for (auto& e : ctx->cache) {
+        if (key_match(e, n, cplx, fb, scales, fn, threads, flags)) {
+            e.last_use = ++ctx->use_clock;
+            *out = e.plan;
+            return FCWT_OK;
+        }
+    }
+    fcwt_plan* p = nullptr;
+    int rc = fcwt_plan_create(ctx, n, cplx, fb, scales, fn, threads, flags, 0, fn, &p);
+    if (rc) return rc;
+    if (ctx->cache.size() >= 4) {
+        auto victim = std::min_element(ctx->cache.begin(), ctx->cache.end(),
+                                       [](const auto& a, const auto& b) { return a.last_use < b.last_use; });
+        fcwt_plan_destroy(victim->plan);
+        ctx->cache.erase(victim);
+    }
+    fcwt_context::CacheEntry e;
+    e.n = n;
+    e.is_complex = cplx;
+    e.fn = fn;
+    e.threads = threads;
+    e.flags = flags;
+    e.fb = fb;
+    e.scales.assign(scales, scales + fn);
+    e.plan = p;
+    e.last_use = ++ctx->use_clock;
+    ctx->cache.push_back(std::move(e));
+    *out = p;
+    return FCWT_OK;
+}
+
+int transform(fcwt_context* ctx, const float* input, int n, int cplx, float fb, const float* scales, int fn,
+              int threads, unsigned flags, void* output, int out_type) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (n < 0 || fn < 0) return fail(FCWT_ERR_INVALID, "negative size");
+    if (n == 0 || fn == 0) return FCWT_OK;
+    if (!scales) return fail(FCWT_ERR_INVALID, "null scales");
+    fcwt_plan* p = nullptr;
+    rc = cached_plan(ctx, n, cplx, fb, scales, fn, threads, flags, &p);
+    if (rc) return rc;
+    return plan_run(p, input, output, out_type);
+}
+
+std::string tune_path(const char* dir, int N, int threads) {
+    std::string d = dir && *dir ? std::string(dir) : std::string(".");
+    if (d.back() != '/') d += '/';
+    return d + "n" + std::to_string(N) + "_t" + std::to_string(threads) + ".wis";
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+int fcwt_version(void) { return 100; }
+
+const char* fcwt_last_error(void) { return g_err.c_str(); }
+
+int fcwt_context_create(int device, fcwt_context** out) {
+    if (!out) return fail(FCWT_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int count = 0;
+    FCWT_CUDA_TRY(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(FCWT_ERR_INVALID, "no such CUDA device");
+    FCWT_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FCWT_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(FCWT_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+    fcwt_context* c = new fcwt_context();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->err_host, sizeof(int));
+    if (e == cudaSuccess) e = fcwt::engine_configure();
+    if (e != cudaSuccess) {
+        if (c->own) cudaStreamDestroy(c->own);
+        if (c->err_host) cudaFreeHost(c->err_host);
+        delete c;
+        return fail(FCWT_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e));
+    }
+    *c->err_host = 0;
+    c->stream = c->own;
+    *out = c;
+    return FCWT_OK;
+}
+
+int fcwt_context_destroy(fcwt_context* ctx) {
+    if (!ctx) return FCWT_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& e : ctx->cache) plan_free(e.plan);
+    ctx->cache.clear();
+    ctx->in_stage.release();
+    ctx->out_stage.release();
+    ctx->tmp.release();
+    ctx->scratch.release();
+    ctx->counters.release();
+    ctx->err.release();
+    if (ctx->err_host) cudaFreeHost(ctx->err_host);
+    for (auto& ev : ctx->ev_used) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    for (auto& ev : ctx->ev_free) {
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return FCWT_OK;
+}
+
+int fcwt_context_set_stream(fcwt_context* ctx, void* stream) {
+    if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return FCWT_OK;
+}
+
+int fcwt_synchronize(fcwt_context* ctx) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    FCWT_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->err_host != 0) {
+        int bits = *ctx->err_host;
+        *ctx->err_host = 0;
+        return fail(FCWT_ERR_DEVICE, "row engine reported error bits " + std::to_string(bits));
+    }
+    return FCWT_OK;
+}
+
+int fcwt_profile_enable(fcwt_context* ctx, int enable) {
+    if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
+    ctx->profiling = enable != 0;
+    return FCWT_OK;
+}
+
+int fcwt_profile_read(fcwt_context* ctx, double* engine_ms, int* engine_launches, int* kernel_launches) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    double total = 0.0;
+    int count = 0;
+    for (auto& ev : ctx->ev_used) {
+        FCWT_CUDA_TRY(cudaEventSynchronize(ev.second));
+        float ms = 0.0f;
+        FCWT_CUDA_TRY(cudaEventElapsedTime(&ms, ev.first, ev.second));
+        total += ms;
+        count++;
+        ctx->ev_free.push_back(ev);
+    }
+    ctx->ev_used.clear();
+    if (engine_ms) *engine_ms = total;
+    if (engine_launches) *engine_launches = count;
+    if (kernel_launches) *kernel_launches = (int)ctx->kernel_launches;
+    ctx->kernel_launches = 0;
+    return FCWT_OK;
+}
+
+int fcwt_find2power(int n) { return fcwt::host::find2power(n); }
+
+int fcwt_scales(int scaletype, int fs, float f0, float f1, int fn, float* out) {
+    if (fn < 0 || (fn > 0 && !out)) return fail(FCWT_ERR_INVALID, "bad scales output");
+    if (scaletype < 0 || scaletype > 2) return fail(FCWT_ERR_INVALID, "unknown scale type");
+    fcwt::host::scales(scaletype, fs, f0, f1, fn, out);
+    return FCWT_OK;
+}
+
+int fcwt_frequencies(const float* scales, int fn, int fs, float* out) {
+    if (fn < 0 || (fn > 0 && (!out || !scales))) return fail(FCWT_ERR_INVALID, "bad arguments");
+    fcwt::host::frequencies(scales, fn, fs, out);
+    return FCWT_OK;
+}
+
+int fcwt_morlet_support(float fb, float scale) { return fcwt::host::morlet_support(fb, scale); }
+
+int fcwt_morlet_time(float fb, float scale, int size, float* real, float* imag) {
+    if (!real || !imag) return fail(FCWT_ERR_INVALID, "null output");
+    fcwt::host::morlet_time(fb, scale, size, real, imag);
+    return FCWT_OK;
+}
+
+int fcwt_morlet_wavelet(float fb, float scale, float* out, int pn) {
+    if (pn < 0 || (pn > 0 && !out)) return fail(FCWT_ERR_INVALID, "bad output");
+    fcwt::host::morlet_wavelet(fb, scale, pn, out);
+    return FCWT_OK;
+}
+
+int fcwt_morlet_mother_host(float fb, int N, float* out) {
+    if (N < 0 || (N > 0 && !out)) return fail(FCWT_ERR_INVALID, "bad output");
+    fcwt::host::mother_table(fb, N, out);
+    return FCWT_OK;
+}
+
+int fcwt_row_truncation(int n, float fb, const float* scales, int fn, int threads, unsigned flags,
+                        int* proc_out, int* lo_out, int* hi_out) {
+    if (fn < 0 || (fn > 0 && (!scales || !proc_out))) return fail(FCWT_ERR_INVALID, "bad arguments");
+    fcwt::SignalPlan sp;
+    std::string err;
+    if (fcwt::plan_signal(n, false, fb, scales, fn, threads, flags, sp, err))
+        return fail(FCWT_ERR_INVALID, err);
+    for (int i = 0; i < fn; i++) {
+        proc_out[i] = sp.rows[(size_t)i].proc;
+        if (lo_out) lo_out[i] = sp.rows[(size_t)i].lo;
+        if (hi_out) hi_out[i] = sp.rows[(size_t)i].hi;
+    }
+    return FCWT_OK;
+}
+
+int fcwt_morlet_mother(fcwt_context* ctx, float fb, int N, float* out) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (N <= 0 || !out) return fail(FCWT_ERR_INVALID, "bad arguments");
+    if (!(fb > 0.0f)) return fail(FCWT_ERR_INVALID, "bandwidth must be positive");
+    if (is_device_pointer(out)) {
+        FCWT_CUDA_TRY(fcwt::launch_mother(fb, N, fcwt::host::mother_norm(), out, ctx->stream));
+        return FCWT_OK;
+    }
+    DevBuf tmp;
+    FCWT_CUDA_TRY(tmp.ensure((size_t)N * sizeof(float)));
+    cudaError_t e = fcwt::launch_mother(fb, N, fcwt::host::mother_norm(), tmp.as<float>(), ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, tmp.p, (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    tmp.release();
+    if (e != cudaSuccess) return fail(FCWT_ERR_CUDA, cudaGetErrorString(e));
+    return FCWT_OK;
+}
+
+int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const float* scales, int fn,
+                     int threads, unsigned flags, int row_begin, int row_end, fcwt_plan** out) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (!out) return fail(FCWT_ERR_INVALID, "null plan output");
+    *out = nullptr;
+    if (fn < 0 || n < 0) return fail(FCWT_ERR_INVALID, "negative size");
+    if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
+    if (row_begin < 0 || row_end > fn || row_begin > row_end)
+        return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
+    fcwt_plan* P = new fcwt_plan();
+    P->ctx = ctx;
+    P->rb = row_begin;
+    P->re = row_end;
+    std::string err;
+    if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sp, err)) {
+        delete P;
+        return fail(FCWT_ERR_INVALID, err);
+    }
+    rc = plan_build(P);
+    if (rc) {
+        std::string keep = g_err;
+        plan_free(P);
+        g_err = keep;
+        return rc;
+    }
+    *out = P;
+    return FCWT_OK;
+}
+
+int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type) {
+    if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    return plan_run(plan, input, output, out_type);
+}
+
+int fcwt_plan_destroy(fcwt_plan* plan) {
+    if (!plan) return FCWT_OK;
+    fcwt_context* ctx = plan->ctx;
+    if (ctx) {
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    plan_free(plan);
+    return FCWT_OK;
+}
+
+int fcwt_cwt(fcwt_context* ctx, const float* input, int n, float fb, const float* scales, int fn, int threads,
+             unsigned flags, void* output, int out_type) {
+    return transform(ctx, input, n, 0, fb, scales, fn, threads, flags, output, out_type);
+}
+
+int fcwt_ccwt(fcwt_context* ctx, const float* input, int n, float fb, const float* scales, int fn,
+              int threads, unsigned flags, void* output, int out_type) {
+    return transform(ctx, input, n, 1, fb, scales, fn, threads, flags, output, out_type);
+}
+
+int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const char* directory) {
+    if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
+    const int log2N = fcwt::host::find2power(n);
+    if (log2N > fcwt::kMaxLog2N) return fail(FCWT_ERR_INVALID, "signal too long");
+    const std::string path = tune_path(directory, 1 << log2N, threads);
+    std::ifstream f(path);
+    if (!f) return fail(FCWT_ERR_IO, "optimization plan '" + path + "' was not found");
+    std::string magic;
+    std::getline(f, magic);
+    if (magic != "fcwt-b200-tune 1") return fail(FCWT_ERR_IO, "optimization plan '" + path + "' is malformed");
+    TuneChoice tc;
+    std::string line;
+    int got = 0;
+    while (std::getline(f, line)) {
+        std::istringstream ls(line);
+        std::string key;
+        long long v;
+        if (!(ls >> key >> v)) continue;
+        if (key == "scratch_mb" && v >= 1 && v <= 4096) {
+            tc.scratch_mb = (int)v;
+            got |= 1;
+        } else if (key == "lag" && v >= 1 && v <= 64) {
+            tc.lag = (int)v;
+            got |= 2;
+        }
+    }
+    if (got != 3) return fail(FCWT_ERR_IO, "optimization plan '" + path + "' is malformed");
+    ctx->tune[log2N] = tc;
+    // cached plans of that size were built with the old choices
+    for (auto it = ctx->cache.begin(); it != ctx->cache.end();) {
+        if (it->plan->sp.log2N == log2N) {
+            fcwt_plan_destroy(it->plan);
+            it = ctx->cache.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    return FCWT_OK;
+}
+
+int fcwt_create_optimization_plan(fcwt_context* ctx, int maxsize, int threads, int level, const char* directory) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (threads < 1) return fail(FCWT_ERR_INVALID, "threads must be >= 1");
+    if (level < 0 || level > 3) return fail(FCWT_ERR_INVALID, "level must be 0..3");
+    const int nt = fcwt::host::find2power(maxsize);
+    if (nt > fcwt::kMaxLog2N) return fail(FCWT_ERR_INVALID, "maxsize too large");
+    for (int i = 11; i <= nt; i++) {
+        const int N = 1 << i;
+        TuneChoice best;
+        if (level > 0 && N > fcwt::kMaxFusedN) {
+            // candidate grid grows with the level
+            std::vector<TuneChoice> cands;
+            const int mbs[] = {16, 32, 64, 96};
+            const int lags[] = {4, 8, 12, 16};
+            const int nm = level == 1 ? 2 : (level == 2 ? 3 : 4);
+            for (int a = 0; a < nm; a++)
+                for (int b = 0; b < nm; b++) cands.push_back({mbs[a + (4 - nm)], lags[b]});
+            // synthetic workload: N samples, 256 log-spaced scales over the band
+            const int fn = 256;
+            std::vector<float> sc((size_t)fn), x((size_t)N);
+            fcwt::host::scales(FCWT_LOGSCALES, 1000, 1.0f, 400.0f, fn, sc.data());
+            for (int t = 0; t < N; t++) x[(size_t)t] = (float)std::sin(0.01 * t) + 0.1f * (float)((t * 7919) % 13);
+            DevBuf din, dout;
+            FCWT_CUDA_TRY(din.ensure((size_t)N * 4));
+            FCWT_CUDA_TRY(dout.ensure((size_t)N * fn * 8));
+            FCWT_CUDA_TRY(cudaMemcpy(din.p, x.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
+            double best_t = 1e30;
+            for (const TuneChoice& tc : cands) {
+                ctx->tune[i] = tc;
+                fcwt_plan* p = nullptr;
+                rc = fcwt_plan_create(ctx, N, 0, 2.0f, sc.data(), fn, threads, FCWT_NORM, 0, fn, &p);
+                if (rc) return rc;
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                rc = plan_run(p, din.p, dout.p, FCWT_OUT_C64);  // warm-up
+                cudaEventRecord(e0, ctx->stream);
+                for (int r = 0; r < 3 && rc == 0; r++) rc = plan_run(p, din.p, dout.p, FCWT_OUT_C64);
+                cudaEventRecord(e1, ctx->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                fcwt_plan_destroy(p);
+                if (rc) return rc;
+                rc = fcwt_synchronize(ctx);
+                if (rc) return rc;
+                if (ms < best_t) {
+                    best_t = ms;
+                    best = tc;
+                }
+            }
+            din.release();
+            dout.release();
+        }
+        ctx->tune[i] = best;
+        const std::string path = tune_path(directory, N, threads);
+        std::ofstream f(path);
+        if (!f) return fail(FCWT_ERR_IO, "cannot write '" + path + "'");
+        f << "fcwt-b200-tune 1\n";
+        f << "N " << N << "\n";
+        f << "threads " << threads << "\n";
+        f << "scratch_mb " << best.scratch_mb << "\n";
+        f << "lag " << best.lag << "\n";
+        if (!f) return fail(FCWT_ERR_IO, "cannot write '" + path + "'");
+    }
+    return FCWT_OK;
+}
+
+}  // extern "C"

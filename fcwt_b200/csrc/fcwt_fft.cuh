@@ -1,0 +1,103 @@
+// Register-resident power-of-two DFTs with compile-time twiddles, plus small
+// complex helpers. Radix-2 decimation in time; the bit-reversal permutation is
+// resolved at compile time (pure register renaming). Trivial rotations (1, ±i,
+// (1±i)/sqrt2 and their negatives) are special-cased so no multiply is spent
+// on them.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fcwt {
+namespace dev {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// cos(2*pi*j/64), j = 0..16
+constexpr float kCos64[17] = {
+    1.000000000e+00f, 9.951847267e-01f, 9.807852804e-01f, 9.569403357e-01f, 9.238795325e-01f,
+    8.819212643e-01f, 8.314696123e-01f, 7.730104534e-01f, 7.071067812e-01f, 6.343932842e-01f,
+    5.555702330e-01f, 4.713967368e-01f, 3.826834324e-01f, 2.902846773e-01f, 1.950903220e-01f,
+    9.801714033e-02f, 0.0f};
+
+// a * exp(SIGN * 2*pi*i * J/64) for 0 <= J < 32.
+template <int J, int SIGN>
+__device__ __forceinline__ float2 rot64(float2 a) {
+    constexpr float r = 7.071067812e-01f;
+    if constexpr (J == 0) {
+        return a;
+    } else if constexpr (J == 16) {
+        return SIGN > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+    } else if constexpr (J == 8) {
+        return SIGN > 0 ? make_float2((a.x - a.y) * r, (a.x + a.y) * r)
+                        : make_float2((a.x + a.y) * r, (a.y - a.x) * r);
+    } else if constexpr (J == 24) {
+        return SIGN > 0 ? make_float2(-(a.x + a.y) * r, (a.x - a.y) * r)
+                        : make_float2((a.y - a.x) * r, -(a.x + a.y) * r);
+    } else {
+        constexpr float c = J <= 16 ? kCos64[J] : -kCos64[32 - J];
+        constexpr float s0 = J <= 16 ? kCos64[16 - J] : kCos64[J - 16];
+        constexpr float s = SIGN > 0 ? s0 : -s0;
+        return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
+}
+
+__host__ __device__ constexpr int ilog2c(int k) { return k <= 1 ? 0 : 1 + ilog2c(k / 2); }
+__host__ __device__ constexpr int brev(int x, int bits) {
+    int r = 0;
+    for (int i = 0; i < bits; i++) r = (r << 1) | ((x >> i) & 1);
+    return r;
+}
+
+template <int K, int SIGN, int LEN, int J>
+__device__ __forceinline__ void dit_stage(float2 (&y)[K]) {
+    if constexpr (J < LEN / 2) {
+#pragma unroll
+        for (int b = 0; b < K; b += LEN) {
+            float2 a = y[b + J];
+            float2 t = rot64<J * (64 / LEN), SIGN>(y[b + J + LEN / 2]);
+            y[b + J] = cadd(a, t);
+            y[b + J + LEN / 2] = csub(a, t);
+        }
+        dit_stage<K, SIGN, LEN, J + 1>(y);
+    }
+}
+
+template <int K, int SIGN, int LEN>
+__device__ __forceinline__ void dit_stages(float2 (&y)[K]) {
+    if constexpr (LEN <= K) {
+        dit_stage<K, SIGN, LEN, 0>(y);
+        dit_stages<K, SIGN, LEN * 2>(y);
+    }
+}
+
+// In-place K-point DFT, natural order in and out:
+//   x[u] <- sum_j x[j] * exp(SIGN * 2*pi*i * j*u / K),  K in {1,2,...,32}.
+template <int K, int SIGN>
+__device__ __forceinline__ void fft_reg(float2 (&x)[K]) {
+    static_assert(K >= 1 && K <= 32 && (K & (K - 1)) == 0, "K must be a power of two <= 32");
+    if constexpr (K > 1) {
+        constexpr int LG = ilog2c(K);
+        float2 y[K];
+#pragma unroll
+        for (int i = 0; i < K; i++) y[i] = x[brev(i, LG)];
+        dit_stages<K, SIGN, 2>(y);
+#pragma unroll
+        for (int i = 0; i < K; i++) x[i] = y[i];
+    }
+}
+
+// w_N^e from the two-level table of a transform length N = 2^log2N:
+// tw[0..1023] = w_N^j, tw[1024 + j] = w_N^{1024 j}. SIGN < 0 conjugates.
+__device__ __forceinline__ float2 tw_lookup(const float2* __restrict__ tw, int log2N, unsigned e) {
+    if (log2N <= 10) return __ldg(tw + (e & ((1u << log2N) - 1)));
+    e &= (1u << log2N) - 1;
+    return cmul(__ldg(tw + (e & 1023u)), __ldg(tw + 1024 + (e >> 10)));
+}
+
+}  // namespace dev
+}  // namespace fcwt

@@ -1,0 +1,488 @@
+// sm_100a kernels of the fCWT transform path.
+//
+//   k_mother      Morlet frequency-domain mother table (Morlet::generate(int),
+//                 src/fcwt/fcwt.cpp:51-67): float operations in the
+//                 reference's order, exp evaluated in float64 then rounded.
+//   k_twiddle     two-level twiddle table w_N^j (float64 sincospi, rounded).
+//   k_fwd_pass    one radix-R Stockham pass of the forward FFT of the
+//                 zero-padded input (replaces fftwf r2c / c2c FORWARD,
+//                 fcwt.cpp:486-500). Only bins < N/2 are consumed later; the
+//                 reference's conjugate mirror (fcwt.cpp:507-510) writes bins
+//                 the Morlet product never reads.
+//   k_row_engine  persistent row engine: daughter multiply (fcwt.cpp:197-311),
+//                 inverse FFT (fcwt.cpp:418-429), normalisation
+//                 (fcwt.cpp:431-445) and crop to n (fcwt.cpp:396-416), fused,
+//                 driven by a work queue of per-row items.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fcwt_fft.cuh"
+#include "fcwt_internal.h"
+
+namespace fcwt {
+namespace dev {
+
+// ------------------------------------------------------------------ tables
+
+__global__ void k_mother(float fb, int N, float norm, float* __restrict__ out) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= N) return;
+    const float two_pi = 2.0f * 3.14159265358979323846f;  // 2*PI in float, as the reference
+    float toradians = __fdiv_rn(two_pi, (float)N);
+    float t = __fmul_rn(__fmul_rn(2.0f, __fmul_rn((float)w, toradians)), fb);
+    t = __fsub_rn(t, __fmul_rn(two_pi, fb));
+    t = __fdiv_rn(-__fmul_rn(t, t), 2.0f);
+    float e = (float)exp((double)t);
+    out[w] = __fmul_rn(norm, e);
+}
+
+// tw[j] = w_N^j for j < 1024; tw[1024 + j] = w_N^{1024 j} for j < max(M, 1).
+// w_N = exp(+2 pi i / N).
+__global__ void k_twiddle(int log2N, float2* __restrict__ tw) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = 1 << log2N;
+    const int M = N >= 1024 ? N / 1024 : 1;
+    if (j >= 1024 + M) return;
+    long long e = j < 1024 ? j : (long long)(j - 1024) * 1024;
+    e &= (long long)N - 1;
+    double s, c;
+    sincospi(2.0 * (double)e / (double)N, &s, &c);
+    tw[j] = make_float2((float)c, (float)s);
+}
+
+// ------------------------------------------------------------- forward FFT
+
+// One Stockham pass (natural order in and out after the last pass):
+//   k = j mod Ns; v_r = in[j + r N/R] * w^{-r k / (Ns R)}; V = DFT_R^-(v);
+//   out[(j - k) R + k + m Ns] = V_m.
+// The first pass reads the caller's signal with implicit zero padding.
+template <int R>
+__global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restrict__ in_r, int n_in,
+                           int first, float2* __restrict__ out, int log2N, int log2Ns,
+                           const float2* __restrict__ tw) {
+    const int N = 1 << log2N;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N / R) return;
+    const int Ns = 1 << log2Ns;
+    const int k = j & (Ns - 1);
+    const int shift = log2N - log2Ns - ilog2c(R);  // N / (Ns R) = 2^shift
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        int idx = j + r * (N / R);
+        float2 a;
+        if (first) {
+            if (idx < n_in)
+                a = in_r ? make_float2(__ldg(in_r + idx), 0.0f) : __ldg(in_c + idx);
+            else
+                a = make_float2(0.0f, 0.0f);
+        } else {
+            a = in_c[idx];
+        }
+        if (r > 0 && k > 0) {
+            float2 w = tw_lookup(tw, log2N, (unsigned)(r * k) << shift);
+            w.y = -w.y;
+            a = cmul(a, w);
+        }
+        v[r] = a;
+    }
+    fft_reg<R, -1>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; m++) out[base + m * Ns] = v[m];
+}
+
+
+// --------------------------------------------------------------- row engine
+
+// Shared-memory layout of the row engine (units of float2).
+constexpr int kRegion0 = kP2 * 17;           // G (fused rows) / transposes / output staging
+constexpr int kZs = kChunk * kMaxK;          // phase-1 input tile
+constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 /*twlo*/ + kP2 /*t2*/;
+constexpr size_t kEngineSmemBytes = (size_t)kSmemFloat2 * sizeof(float2);
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait until *p >= target. Returns false (and sets err) on timeout or
+// when another CTA already reported an error.
+__device__ bool wait_counter(const unsigned* p, unsigned target, int* err) {
+    unsigned it = 0;
+    while (ld_acquire(p) < target) {
+        if (*((volatile int*)err) != 0) return false;
+        if (++it > (1u << 22)) {
+            atomicOr(err, kErrWaitTimeout);
+            return false;
+        }
+        __nanosleep(200);
+    }
+    return true;
+}
+
+// Daughter weight of bin q (reference: mother[(int)min(N-1, step*q)] for the
+// row that last wrote bin q into O1; 0 if no row did).
+__device__ __forceinline__ float bin_weight(const RowDesc& R, const float* __restrict__ mother,
+                                           const float* __restrict__ pool, float nm1, int q) {
+    float s;
+    if (q < R.proc)
+        s = R.step;
+    else if (R.stale >= 0)
+        s = __ldg(pool + R.stale + q);
+    else
+        return 0.0f;
+    if (!(s > 0.0f)) return 0.0f;
+    int w = (int)fminf(nm1, __fmul_rn(s, (float)q));
+    return __ldg(mother + w);
+}
+
+template <int OT>
+__device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
+    if constexpr (OT == OUT_C64) {
+        __stcs(reinterpret_cast<float2*>(base) + idx, v);
+    } else if constexpr (OT == OUT_BF16) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        __stcs(reinterpret_cast<unsigned*>(base) + idx, *reinterpret_cast<unsigned*>(&h));
+    } else {
+        __half2 h = __floats2half2_rn(v.x, v.y);
+        __stcs(reinterpret_cast<unsigned*>(base) + idx, *reinterpret_cast<unsigned*>(&h));
+    }
+}
+
+// Phase 1 of one chunk of kChunk k2 values of a row (see fcwt_internal.h):
+// loads Z = Ihat * W into the tile zs[k1][k2], then every (k2, v) task runs a
+// K-point DFT and writes G[c][k2] (c = v + R u) with its twiddle.
+template <int K, bool TO_GLOBAL>
+__device__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
+                             float2* __restrict__ zs, const float2* __restrict__ twlo,
+                             float2* __restrict__ gdst) {
+    const int tid = threadIdx.x;
+    const int log2N = S.log2N;
+    const int N = 1 << log2N;
+    const int M = N >> kLog2P2;
+    const int Rr = M / K;
+    const float nm1 = (float)N - 1.0f;
+    const float2* __restrict__ X = S.X;
+    // (a) input tile
+    for (int idx = tid; idx < K * kChunk; idx += kThreads) {
+        const int k1 = idx / kChunk;
+        const int kl = idx - k1 * kChunk;
+        const int q = R.L + k2_0 + kl + kP2 * k1;
+        float2 z = make_float2(0.0f, 0.0f);
+        if (q >= R.lo && q < R.hi) {
+            float m = bin_weight(R, S.mother, pool, nm1, q);
+            float2 xv = __ldg(X + q);
+            z = make_float2(xv.x * m, xv.y * m);
+        }
+        zs[idx] = z;
+    }
+    __syncthreads();
+    // (b) tasks
+    const float2* __restrict__ twhi = S.tw + kP2;
+    for (int t = tid; t < kChunk * Rr; t += kThreads) {
+        const int kl = t % kChunk;
+        const int v = t / kChunk;
+        float2 z[K];
+#pragma unroll
+        for (int k1 = 0; k1 < K; k1++) z[k1] = zs[k1 * kChunk + kl];
+        if (v != 0) {
+#pragma unroll
+            for (int k1 = 1; k1 < K; k1++) z[k1] = cmul(z[k1], __ldg(twhi + v * k1));
+        }
+        fft_reg<K, +1>(z);
+        const unsigned k2L = (unsigned)(k2_0 + kl + R.L);
+        const int k2 = k2_0 + kl;
+#pragma unroll
+        for (int u = 0; u < K; u++) {
+            const int c = v + Rr * u;
+            const unsigned e = (k2L * (unsigned)c) & (unsigned)(N - 1);
+            const float2 w = cmul(twlo[e & 1023u], __ldg(twhi + (e >> 10)));
+            const float2 g = cmul(z[u], w);
+            if constexpr (TO_GLOBAL)
+                __stcg(gdst + (size_t)c * kP2 + k2, g);
+            else
+                gdst[c * kP2 + k2] = g;
+        }
+    }
+    __syncthreads();
+}
+
+template <bool TO_GLOBAL>
+__device__ void phase1_chunk_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool,
+                                      int k2_0, float2* zs, const float2* twlo, float2* gdst) {
+    switch (K) {
+        case 1: phase1_chunk<1, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        case 2: phase1_chunk<2, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        case 4: phase1_chunk<4, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        case 8: phase1_chunk<8, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        case 16: phase1_chunk<16, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        default: phase1_chunk<32, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+    }
+}
+
+// Warp-level 1024-point DFT (sign +): on entry lane l holds x[m] = G[l + 32 m];
+// on exit lane l holds x[h] = Y[l + 32 h]. tbuf: 32*33 float2 of this warp.
+__device__ __forceinline__ void dft1024_warp(float2 (&x)[32], int lane, float2* __restrict__ tbuf,
+                                             const float2* __restrict__ t2) {
+    fft_reg<32, +1>(x);
+#pragma unroll
+    for (int a = 1; a < 32; a++) x[a] = cmul(x[a], t2[a * 32 + lane]);
+#pragma unroll
+    for (int a = 0; a < 32; a++) tbuf[a * 33 + lane] = x[a];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) x[k] = tbuf[lane * 33 + k];
+    __syncwarp();
+    fft_reg<32, +1>(x);
+}
+
+template <int OT>
+__global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
+    extern __shared__ float2 smem[];
+    float2* region0 = smem;
+    float2* zs = smem + kRegion0;
+    float2* twlo = zs + kZs;
+    float2* t2 = twlo + kP2;
+    __shared__ int s_item;
+    __shared__ int s_log2N;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+
+    // t2[a*32 + l] = w_1024^{a l}
+    for (int j = tid; j < kP2; j += kThreads) {
+        const int a = j >> 5, l = j & 31;
+        double s, c;
+        sincospi(2.0 * (double)((a * l) & 1023) / 1024.0, &s, &c);
+        t2[j] = make_float2((float)c, (float)s);
+    }
+    if (tid == 0) s_log2N = -1;
+    __syncthreads();
+
+    unsigned* a_done = P.counters + 1;
+    unsigned* b_done = P.counters + 1 + P.n_rows;
+
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(P.counters, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= P.n_items) break;
+        const Item item = P.items[it];
+        const RowDesc R = P.rows[item.row];
+        const SigDesc S = P.sigs[R.sig];
+        const int log2N = S.log2N;
+        const int N = 1 << log2N;
+        const int n = S.n;
+        void* outb = P.outs[R.out_buf];
+
+        // twiddle table of this N into SMEM (first 1024 entries)
+        if (s_log2N != log2N) {
+            for (int j = tid; j < kP2; j += kThreads) twlo[j] = S.tw[j];
+            __syncthreads();
+            if (tid == 0) s_log2N = log2N;
+        }
+
+        if (item.type == ITEM_SMALL) {
+            // N < 1024: direct DFT over the row's nonzero bins.
+            const int lo = R.lo, hi = R.hi;
+            const float nm1 = (float)N - 1.0f;
+            for (int q = lo + tid; q < hi; q += kThreads) {
+                float m = bin_weight(R, S.mother, P.stale_pool, nm1, q);
+                float2 xv = __ldg(S.X + q);
+                zs[q - lo] = make_float2(xv.x * m, xv.y * m);
+            }
+            __syncthreads();
+            for (int t = tid; t < n; t += kThreads) {
+                float2 acc = make_float2(0.0f, 0.0f);
+                for (int q = lo; q < hi; q++) {
+                    const float2 w = twlo[(q * t) & (N - 1)];
+                    const float2 z = zs[q - lo];
+                    acc.x += z.x * w.x - z.y * w.y;
+                    acc.y += z.x * w.y + z.y * w.x;
+                }
+                store_out<OT>(outb, R.out_off + t, cscale(acc, R.out_scale));
+            }
+        } else if (item.type == ITEM_FUSED) {
+            // whole row in this CTA: phase 1 into SMEM, then phase 2
+            const int M = N >> kLog2P2;
+            for (int k2_0 = 0; k2_0 < kP2; k2_0 += kChunk)
+                phase1_chunk_dispatch<false>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, region0);
+            float2 x[32];
+            if (warp < M) {
+#pragma unroll
+                for (int m = 0; m < 32; m++) x[m] = region0[warp * kP2 + lane + 32 * m];
+            }
+            __syncthreads();
+            if (warp < M) dft1024_warp(x, lane, region0 + warp * (32 * 33), t2);
+            __syncthreads();
+            if (warp < M) {
+#pragma unroll
+                for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * 17 + warp] = x[h];
+            }
+            __syncthreads();
+            const int log2M = log2N - kLog2P2;
+            for (int t = tid; t < n; t += kThreads) {
+                const int c = t & (M - 1);
+                const int a = t >> log2M;
+                store_out<OT>(outb, R.out_off + t, cscale(region0[a * 17 + c], R.out_scale));
+            }
+        } else if (item.type == ITEM_PHASE1) {
+            if (tid == 0) {
+                s_ok = 1;
+                if (R.wait_row >= 0)
+                    s_ok = wait_counter(b_done + R.wait_row, (unsigned)P.rows[R.wait_row].n_b, P.err) ? 1 : 0;
+            }
+            __syncthreads();
+            if (s_ok) {
+                float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
+                const int k2_0 = item.part * kChunk;
+                phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, G);
+                if (tid == 0) {
+                    __threadfence();
+                    red_release_add(a_done + item.row, 1u);
+                }
+            }
+        } else if (item.type == ITEM_PHASE2) {
+            if (tid == 0) s_ok = wait_counter(a_done + item.row, (unsigned)R.n_a, P.err) ? 1 : 0;
+            __syncthreads();
+            if (s_ok) {
+                const int M = N >> kLog2P2;
+                const float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
+                const int c0 = item.part * kGroupCols;
+                const int c = c0 + warp;
+                float2 x[32];
+#pragma unroll
+                for (int m = 0; m < 32; m++) x[m] = __ldcg(G + (size_t)c * kP2 + lane + 32 * m);
+                dft1024_warp(x, lane, region0 + warp * (32 * 33), t2);
+                __syncthreads();
+#pragma unroll
+                for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * 17 + warp] = x[h];
+                __syncthreads();
+                for (int idx = tid; idx < kGroupCols * kP2; idx += kThreads) {
+                    const int w = idx & (kGroupCols - 1);
+                    const int a = idx >> 4;
+                    const long long t = (long long)c0 + w + (long long)M * a;
+                    if (t < n) store_out<OT>(outb, R.out_off + t, cscale(region0[a * 17 + w], R.out_scale));
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    __threadfence();
+                    red_release_add(b_done + item.row, 1u);
+                }
+            }
+        } else {
+            if (tid == 0) atomicOr(P.err, kErrBadItem);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace dev
+
+// ------------------------------------------------------------ launch glue
+
+size_t engine_smem_bytes() { return dev::kEngineSmemBytes; }
+
+cudaError_t launch_mother(float fb, int N, float norm, float* out, cudaStream_t st) {
+    const int tb = 256;
+    dev::k_mother<<<(N + tb - 1) / tb, tb, 0, st>>>(fb, N, norm, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st) {
+    const int N = 1 << log2N;
+    const int M = N >= 1024 ? N / 1024 : 1;
+    const int total = 1024 + M;
+    dev::k_twiddle<<<(total + 255) / 256, 256, 0, st>>>(log2N, tw);
+    return cudaGetLastError();
+}
+
+// Forward FFT of the zero-padded input into `out` (N complex values), using
+// `tmp` (N complex) as the ping-pong buffer.
+cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
+                           float2* out, float2* tmp, cudaStream_t st, int* n_kernels) {
+    const int N = 1 << log2N;
+    *n_kernels = 0;
+    if (log2N == 0) {
+        // N == 1: the DFT is the identity (one sample or none).
+        cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float2), st);
+        if (e != cudaSuccess) return e;
+        if (n >= 1) {
+            if (in_r)
+                e = cudaMemcpy2DAsync(out, sizeof(float2), in_r, sizeof(float), sizeof(float), 1,
+                                      cudaMemcpyDeviceToDevice, st);
+            else
+                e = cudaMemcpyAsync(out, in_c, sizeof(float2), cudaMemcpyDeviceToDevice, st);
+        }
+        return e;
+    }
+    // choose the radix sequence: 16s, then one smaller pass
+    int radices[32];
+    int np = 0, rem = log2N;
+    while (rem >= 4) {
+        radices[np++] = 16;
+        rem -= 4;
+    }
+    if (rem == 3) radices[np++] = 8;
+    if (rem == 2) radices[np++] = 4;
+    if (rem == 1) radices[np++] = 2;
+    // ping-pong so that the last pass lands in `out`
+    float2* bufs[2] = {out, tmp};
+    int cur = (np % 2 == 1) ? 0 : 1;
+    const float2* src_c = in_c;
+    const float* src_r = in_r;
+    int log2Ns = 0;
+    for (int p = 0; p < np; p++) {
+        const int R = radices[p];
+        float2* dst = bufs[cur];
+        const int threads = N / R;
+        const int tb = threads < 256 ? threads : 256;
+        const int grid = (threads + tb - 1) / tb;
+        const int first = p == 0 ? 1 : 0;
+        switch (R) {
+            case 16: dev::k_fwd_pass<16><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2N, log2Ns, tw); break;
+            case 8: dev::k_fwd_pass<8><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2N, log2Ns, tw); break;
+            case 4: dev::k_fwd_pass<4><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2N, log2Ns, tw); break;
+            default: dev::k_fwd_pass<2><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2N, log2Ns, tw); break;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        (*n_kernels)++;
+        src_c = dst;
+        src_r = nullptr;
+        log2Ns += dev::ilog2c(R);
+        cur ^= 1;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t engine_configure() {
+    cudaError_t e;
+    e = cudaFuncSetAttribute(dev::k_row_engine<OUT_C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kEngineSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(dev::k_row_engine<OUT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kEngineSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(dev::k_row_engine<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dev::kEngineSmemBytes);
+}
+
+cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st) {
+    switch (p.out_type) {
+        case OUT_BF16: dev::k_row_engine<OUT_BF16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
+        case OUT_F16: dev::k_row_engine<OUT_F16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
+        default: dev::k_row_engine<OUT_C64><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace fcwt

@@ -1,0 +1,137 @@
+/*
+ * fcwt_b200.h — C ABI of the B200-native fCWT transform path.
+ *
+ * Plain C types only: pointers, sizes and status codes. Every entry point
+ * returns FCWT_OK (0) or an FCWT_ERR_* code; fcwt_last_error() returns a
+ * message for the calling thread's last failure.
+ *
+ * Signal and output pointers may be host or device memory (detected per call).
+ * With host pointers the call copies in and out and returns when the output is
+ * written. With device pointers the call only enqueues work on the context's
+ * stream; fcwt_synchronize() waits for it and reports device-side errors.
+ *
+ * Each entry point names the reference interface it replaces
+ * (reference = fastlib/fCWT, paths inside that project).
+ */
+#ifndef FCWT_B200_H
+#define FCWT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes */
+#define FCWT_OK 0
+#define FCWT_ERR_INVALID 1     /* bad argument (size, pointer, scale, flag)            */
+#define FCWT_ERR_CUDA 2        /* CUDA runtime error                                   */
+#define FCWT_ERR_NOMEM 3       /* device or host allocation failed                     */
+#define FCWT_ERR_UNSUPPORTED 4 /* valid request outside what this build implements     */
+#define FCWT_ERR_DEVICE 5      /* a kernel reported an error (e.g. a bounded wait expired) */
+#define FCWT_ERR_IO 6          /* plan file could not be read or written               */
+
+/* ---- scale distributions: same values as enum SCALETYPE, src/fcwt/fcwt.h:65 */
+#define FCWT_LINSCALES 0
+#define FCWT_LOGSCALES 1
+#define FCWT_LINFREQS 2
+
+/* ---- transform flags */
+#define FCWT_NORM (1u << 0)           /* divide by N: FCWT(..., use_normalization=true) */
+#define FCWT_SCALAR_TRUNC (1u << 1)   /* truncation rule of the reference's non-AVX build */
+#define FCWT_EXACT_SUPPORT (1u << 2)  /* also evaluate bins whose weight is < 2^-44 of the peak */
+
+/* ---- output element types */
+#define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
+#define FCWT_OUT_BF16 1  /* interleaved bfloat16 (re, im), 4 bytes per coefficient */
+#define FCWT_OUT_F16 2   /* interleaved float16 (re, im), 4 bytes per coefficient  */
+
+typedef struct fcwt_context fcwt_context;
+typedef struct fcwt_plan fcwt_plan;
+
+/* ---- library / context */
+int fcwt_version(void);
+const char* fcwt_last_error(void);
+/* One context per device and caller thread; it owns a stream and workspace.
+ * Calls on one context are not reentrant. */
+int fcwt_context_create(int device, fcwt_context** ctx);
+int fcwt_context_destroy(fcwt_context* ctx);
+/* Use an external cudaStream_t (passed as void*); NULL restores the own stream. */
+int fcwt_context_set_stream(fcwt_context* ctx, void* cuda_stream);
+/* Wait for all work of the context and report device-side errors. */
+int fcwt_synchronize(fcwt_context* ctx);
+
+/* Profiling: when enabled, every transform of the context records CUDA events
+ * around its row-engine launch (on the context's stream). */
+int fcwt_profile_enable(fcwt_context* ctx, int enable);
+/* Waits for the recorded launches; returns their summed device time in ms,
+ * the number of row-engine launches, and the number of kernels this library
+ * launched since the previous read (counters reset on read). */
+int fcwt_profile_read(fcwt_context* ctx, double* engine_ms, int* engine_launches, int* kernel_launches);
+
+/* ---- host-side helpers (no GPU needed) */
+/* find2power, src/fcwt/fcwt.h:154-165 */
+int fcwt_find2power(int n);
+/* Scales::Scales(wavelet, st, fs, f0, f1, fn) + getScales, src/fcwt/fcwt.cpp:111-158 */
+int fcwt_scales(int scaletype, int fs, float f0, float f1, int fn, float* scales_out);
+/* Scales::getFrequencies, src/fcwt/fcwt.cpp:133-137 */
+int fcwt_frequencies(const float* scales, int fn, int fs, float* freqs_out);
+/* Morlet::getSupport, src/fcwt/fcwt.h:88 */
+int fcwt_morlet_support(float fb, float scale);
+/* Morlet::generate(real, imag, size, scale), src/fcwt/fcwt.cpp:68-84
+ * (real/imag must hold 2*fcwt_morlet_support(fb, scale)+1 floats) */
+int fcwt_morlet_time(float fb, float scale, int size, float* real, float* imag);
+/* Morlet::getWavelet, src/fcwt/fcwt.cpp:86-105 (pn interleaved complex) */
+int fcwt_morlet_wavelet(float fb, float scale, float* out_interleaved, int pn);
+/* Morlet::generate(int) on the host, src/fcwt/fcwt.cpp:51-67 */
+int fcwt_morlet_mother_host(float fb, int N, float* mother_out);
+/* Per-row truncation length of daughter_wavelet_multiplication,
+ * src/fcwt/fcwt.cpp:197-311 (proc_out: fn ints), and the bin window the
+ * device engine evaluates for Morlet(fb) (lo_out/hi_out may be NULL). */
+int fcwt_row_truncation(int n, float fb, const float* scales, int fn, int threads, unsigned flags,
+                        int* proc_out, int* lo_out, int* hi_out);
+
+/* ---- device: mother table
+ * Morlet::generate(int), src/fcwt/fcwt.cpp:51-67, computed by a kernel. */
+int fcwt_morlet_mother(fcwt_context* ctx, float fb, int N, float* mother_out);
+
+/* ---- device: transforms
+ * FCWT::cwt(float* input, int n, complex<float>* output, Scales*) and the
+ * (input, n, scales, output, n1, n2) overload, src/fcwt/fcwt.cpp:532-543,
+ * with FCWT(Morlet(fb), threads, optplans, norm) (src/fcwt/fcwt.h:116-120):
+ * output row i (of fn) holds the n coefficients of scales[i]. */
+int fcwt_cwt(fcwt_context* ctx, const float* input, int n, float fb, const float* scales, int fn,
+             int threads, unsigned flags, void* output, int out_type);
+/* FCWT::cwt(complex<float>* input, ...), src/fcwt/fcwt.cpp:536-547 (`ccwt`);
+ * input is n interleaved complex values. */
+int fcwt_ccwt(fcwt_context* ctx, const float* input, int n, float fb, const float* scales, int fn,
+              int threads, unsigned flags, void* output, int out_type);
+
+/* Reusable plan (the FFTW-plan analogue): everything that depends only on the
+ * shape, scales and flags is computed once. Rows [row_begin, row_end) of the
+ * fn scales are produced (row sharding); the stale-bin semantics still follow
+ * all fn rows. */
+int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const float* scales, int fn,
+                     int threads, unsigned flags, int row_begin, int row_end, fcwt_plan** plan);
+int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type);
+int fcwt_plan_destroy(fcwt_plan* plan);
+
+/* ---- tuning files
+ * FCWT::create_FFT_optimization_plan(maxsize, flags), src/fcwt/fcwt.cpp:313-374:
+ * for N = 2^11 .. 2^ceil(log2 maxsize), times the engine's scheduling
+ * choices and writes "n<N>_t<threads>.wis" into `directory` (NULL: current
+ * directory). level 0..3 mirrors FFTW_ESTIMATE/MEASURE/PATIENT/EXHAUSTIVE. */
+int fcwt_create_optimization_plan(fcwt_context* ctx, int maxsize, int threads, int level,
+                                  const char* directory);
+/* FCWT::load_FFT_optimization_plan, src/fcwt/fcwt.cpp:376-393: use the
+ * choices stored for (N, threads) by later transforms of this context.
+ * Returns FCWT_ERR_IO when the file is missing or malformed (the context then
+ * keeps its defaults). */
+int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const char* directory);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FCWT_B200_H */

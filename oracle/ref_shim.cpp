@@ -1,0 +1,78 @@
+// C entry points over the reference fCWT C++ classes, so that Python (ctypes)
+// can drive the reference's own CPU path (FFTW + AVX) as the parity oracle and
+// as the timed CPU baseline.
+//
+// This file is test infrastructure. It is compiled together with the
+// reference's src/fcwt/fcwt.cpp (never copied) by oracle/build_ref.sh into
+// oracle/_ref/libfcwt_ref.so. Nothing in the product links or loads it.
+//
+// Each function mirrors one reference call sequence:
+//   ref_scales      -> Scales::Scales + Scales::getScales      (src/fcwt/fcwt.cpp:111-158)
+//   ref_frequencies -> Scales::getFrequencies                  (src/fcwt/fcwt.cpp:133-137)
+//   ref_mother      -> Morlet::generate(int)                   (src/fcwt/fcwt.cpp:51-67)
+//   ref_wavelet     -> Morlet::getWavelet                      (src/fcwt/fcwt.cpp:86-105)
+//   ref_cwt         -> FCWT::cwt (real or complex input)       (src/fcwt/fcwt.cpp:447-548)
+//   ref_create_plan -> FCWT::create_FFT_optimization_plan      (src/fcwt/fcwt.cpp:313-374)
+#include "fcwt.h"
+
+#include <cstring>
+#include <string>
+
+extern "C" {
+
+int ref_find2power(int n) { return find2power(n); }
+
+void ref_scales(float fb, int scaletype, int fs, float f0, float f1, int fn, float* out) {
+    Morlet m(fb);
+    Scales s(&m, (SCALETYPE)scaletype, fs, f0, f1, fn);
+    s.getScales(out, fn);
+    free(s.scales);
+}
+
+void ref_frequencies(float fb, int scaletype, int fs, float f0, float f1, int fn, float* out) {
+    Morlet m(fb);
+    Scales s(&m, (SCALETYPE)scaletype, fs, f0, f1, fn);
+    s.getFrequencies(out, fn);
+    free(s.scales);
+}
+
+void ref_mother(float fb, int N, float* out) {
+    Morlet m(fb);
+    m.generate(N);
+    std::memcpy(out, m.mother, sizeof(float) * (size_t)N);
+}
+
+int ref_support(float fb, float scale) {
+    Morlet m(fb);
+    return m.getSupport(scale);
+}
+
+void ref_wavelet(float fb, float scale, float* out_interleaved, int pn) {
+    Morlet m(fb);
+    m.getWavelet(scale, reinterpret_cast<std::complex<float>*>(out_interleaved), pn);
+}
+
+// Runs the reference transform with an explicit scales array. The Scales
+// object is built with LOGSCALES and its public `scales` array is then
+// overwritten, which is how the reference API lets a caller pass any grid.
+void ref_cwt(const void* input, int n, int is_complex, float fb, const float* scales, int fn,
+             int fs, int threads, int optplans, int norm, void* output) {
+    Morlet m(fb);
+    Scales s(&m, FCWT_LOGSCALES, fs, 1.0f, 2.0f, fn);
+    std::memcpy(s.scales, scales, sizeof(float) * (size_t)fn);
+    FCWT f(&m, threads, optplans != 0, norm != 0);
+    if (is_complex) {
+        f.cwt((std::complex<float>*)input, n, (std::complex<float>*)output, &s);
+    } else {
+        f.cwt((float*)input, n, (std::complex<float>*)output, &s);
+    }
+    free(s.scales);
+}
+
+void ref_create_plan(float fb, int threads, int maxsize, const char* flag) {
+    Morlet m(fb);
+    FCWT f(&m, threads, true, true);
+    f.create_FFT_optimization_plan(maxsize, std::string(flag));
+}
+
+}  // extern "C"
