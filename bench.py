@@ -193,6 +193,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-runs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fn", type=int, default=FN,
+                    help="number of rows; values other than 3000 are for profiling captures only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -221,11 +223,12 @@ def main():
     dev = local_rank
     x = make_signal(1234 + rank)
     morl = fcwt.Morlet(SIGMA)
-    sc = fcwt.Scales(morl, fcwt.FCWT_LINFREQS, FS, F0, F1, FN)
+    fn = args.fn
+    sc = fcwt.Scales(morl, fcwt.FCWT_LINFREQS, FS, F0, F1, fn)
     plan = fcwt.Plan(N_SAMPLES, sc, fb=SIGMA, threads=1, norm=True, device=dev)
     N = 1 << _lib.load().fcwt_find2power(N_SAMPLES)
     xd = torch.from_numpy(x).to(f"cuda:{dev}")
-    out = torch.empty((FN, N_SAMPLES), dtype=torch.complex64, device=f"cuda:{dev}")
+    out = torch.empty((fn, N_SAMPLES), dtype=torch.complex64, device=f"cuda:{dev}")
     stream = torch.cuda.current_stream(dev)
     ctx = plan.ctx
 
@@ -265,14 +268,14 @@ def main():
     else:
         eng_avg = eng_ms / max(eng_n, 1)
     ms_step = ms_total / args.steps
-    points = N_SAMPLES * FN
+    points = N_SAMPLES * fn
     value = world * points * args.steps / (ms_total / 1e3)
 
     # ---- e2e: reference-facing call with host buffers (pinned)
     e2e = None
     if args.e2e_steps > 0:
         xin = torch.from_numpy(x).pin_memory()
-        hout = torch.empty((FN, N_SAMPLES), dtype=torch.complex64, pin_memory=True)
+        hout = torch.empty((fn, N_SAMPLES), dtype=torch.complex64, pin_memory=True)
         xin_np, hout_np = xin.numpy(), hout.numpy()
         f = fcwt.FCWT(morl, 1, False, True, device=dev)
         f.cwt(xin_np, sc, hout_np)  # warm
@@ -311,13 +314,14 @@ def main():
     if rank != 0:
         return
     peak, peak_kind = load_peaks()
-    algo = algorithmic_bytes(N_SAMPLES, FN, N)
+    algo = algorithmic_bytes(N_SAMPLES, fn, N)
     achieved = algo / (eng_avg / 1e3) / 1e9
     line = {
         "metric": "scalogram points/s", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": N_SAMPLES, "N": N, "fn": FN, "fs": FS, "f0": F0, "f1": F1,
+        "config": {"workload": WORKLOAD if fn == FN else WORKLOAD.replace("fn=3000", f"fn={fn}"),
+                   "n": N_SAMPLES, "N": N, "fn": fn, "fs": FS, "f0": F0, "f1": F1,
                    "sigma": SIGMA, "scaling": "LINFREQS", "threads_param": 1, "out": "complex64",
                    "l2": "each step writes a 2.4 GB output (> 126 MB L2); no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -70,7 +70,7 @@ class FcwtError(RuntimeError):
 
 
 _lib = None
-_lock = threading.Lock()
+_lock = threading.RLock()
 
 
 def load() -> ctypes.CDLL:
@@ -125,7 +125,16 @@ class Context:
             pass
 
     def set_stream(self, stream_ptr: int | None) -> None:
-        call("fcwt_context_set_stream", self.handle, ctypes.c_void_p(stream_ptr or 0))
+        """stream_ptr: a cudaStream_t value; 0 is the legacy default stream
+        (what torch reports for its default stream); None restores the
+        context's own stream."""
+        if stream_ptr is None:
+            h = 0
+        elif stream_ptr == 0:
+            h = 1  # cudaStreamLegacy
+        else:
+            h = stream_ptr
+        call("fcwt_context_set_stream", self.handle, ctypes.c_void_p(h))
 
     def synchronize(self) -> None:
         call("fcwt_synchronize", self.handle)

@@ -335,8 +335,9 @@ class Plan:
         _check_host_output(out, self.n_rows, self.n, out_type)
         _lib.call("fcwt_plan_execute", self.handle, _ptr(xin), _ptr(out), out_type)
 
-    def execute_ptr(self, x_ptr: int, out_ptr: int, out_type: int = FCWT_OUT_C64, stream_ptr: int = 0) -> None:
-        """Raw-pointer form (device or host pointers)."""
+    def execute_ptr(self, x_ptr: int, out_ptr: int, out_type: int = FCWT_OUT_C64, stream_ptr: int | None = None) -> None:
+        """Raw-pointer form (device or host pointers); stream_ptr None = the
+        context's own stream, 0 = legacy default stream."""
         self.ctx.set_stream(stream_ptr)
         try:
             _lib.call("fcwt_plan_execute", self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(out_ptr), out_type)

@@ -23,6 +23,7 @@ cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st);
 cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
                            float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
 cudaError_t engine_configure();
+cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
 }  // namespace fcwt
 
@@ -97,6 +98,7 @@ struct fcwt_context {
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     int num_sms = 0;
+    int engine_ctas = 0;  // persistent grid of the row engine
     DevBuf in_stage, out_stage, tmp, scratch, counters, err;
     int* err_host = nullptr;  // pinned mirror of the device error word
     TuneChoice tune[fcwt::kMaxLog2N + 1];
@@ -308,7 +310,7 @@ int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
     ep.outs[0] = dout;
     ep.out_type = out_type;
     ep.err = ctx->err.as<int>();
-    const int grid = std::max(1, std::min(P->n_items, ctx->num_sms));
+    const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (ctx->profiling) {
         if (!ctx->ev_free.empty()) {
@@ -421,6 +423,9 @@ int fcwt_context_create(int device, fcwt_context** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&c->err_host, sizeof(int));
     if (e == cudaSuccess) e = fcwt::engine_configure();
+    int per_sm = 0;
+    if (e == cudaSuccess) e = fcwt::engine_blocks_per_sm(&per_sm);
+    c->engine_ctas = std::max(1, per_sm) * c->num_sms;
     if (e != cudaSuccess) {
         if (c->own) cudaStreamDestroy(c->own);
         if (c->err_host) cudaFreeHost(c->err_host);

@@ -27,11 +27,11 @@ namespace fcwt {
 constexpr int kP2 = 1024;          // phase-2 transform length
 constexpr int kLog2P2 = 10;
 constexpr int kMaxLog2N = 23;      // N <= 8M samples
-constexpr int kMaxFusedN = 16384;  // rows of N <= this run whole inside one CTA
-constexpr int kThreads = 512;      // threads per CTA of the row engine
-constexpr int kChunk = 128;        // phase-1 k2 values handled per SMEM round
+constexpr int kMaxFusedN = 8192;   // rows of N <= this run whole inside one CTA
+constexpr int kThreads = 256;      // threads per CTA of the row engine (2 CTAs per SM)
+constexpr int kChunk = 64;         // phase-1 k2 values per work item
 constexpr int kMaxK = 32;          // phase-1 transform length held in registers
-constexpr int kGroupCols = 16;     // phase-2 columns per work item
+constexpr int kGroupCols = 8;      // phase-2 columns per work item (one per warp)
 constexpr int kMaxOuts = 1024;     // output buffers per launch
 
 // One input signal of a launch (a batch may hold several).

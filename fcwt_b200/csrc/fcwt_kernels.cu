@@ -97,11 +97,19 @@ __global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restr
 
 // --------------------------------------------------------------- row engine
 
-// Shared-memory layout of the row engine (units of float2).
-constexpr int kRegion0 = kP2 * 17;           // G (fused rows) / transposes / output staging
-constexpr int kZs = kChunk * kMaxK;          // phase-1 input tile
-constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 /*twlo*/ + kP2 /*t2*/;
+// Shared-memory layout of the row engine, per CTA (units of float2):
+//   region0: G of a fused row (<= 8192) / per-warp transposes (8 x 32x33) /
+//            output staging [1024][9] of 8 columns
+//   zs:      phase-1 input tile [K][kChunk]
+//   twlo:    w_N^j, j < 1024, of the current N
+//   t2:      w_1024^{a l} at [a*32 + l]
+constexpr int kStagePitch = kGroupCols + 1;
+constexpr int kRegion0 = kP2 * kStagePitch;
+constexpr int kZs = kChunk * kMaxK;
+constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 + kP2;
 constexpr size_t kEngineSmemBytes = (size_t)kSmemFloat2 * sizeof(float2);
+static_assert(kRegion0 >= kMaxFusedN, "fused rows keep G in region0");
+static_assert(kRegion0 >= (kThreads / 32) * 32 * 33, "per-warp transposes live in region0");
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -111,18 +119,28 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
-// Bounded wait until *p >= target. Returns false (and sets err) on timeout or
-// when another CTA already reported an error.
+// Bounded wait until *p >= target: gives up after kWaitLimitNs of wall time
+// (or when another CTA already reported an error) and returns false; the
+// timeout is recorded in *err.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+
 __device__ bool wait_counter(const unsigned* p, unsigned target, int* err) {
+    if (ld_acquire(p) >= target) return true;
+    const unsigned long long t0 = global_ns();
     unsigned it = 0;
     while (ld_acquire(p) < target) {
         if (*((volatile int*)err) != 0) return false;
-        if (++it > (1u << 22)) {
+        if ((++it & 63u) == 0 && global_ns() - t0 > kWaitLimitNs) {
             atomicOr(err, kErrWaitTimeout);
             return false;
         }
-        __nanosleep(200);
+        __nanosleep(256);
     }
     return true;
 }
@@ -143,6 +161,16 @@ __device__ __forceinline__ float bin_weight(const RowDesc& R, const float* __res
     return __ldg(mother + w);
 }
 
+// Z[q] = Ihat[q] * W[q] * out_scale. out_scale is 1 or 1/N, a power of two,
+// so scaling the weight is exact and equals scaling the output.
+__device__ __forceinline__ float2 bin_value(const RowDesc& R, const SigDesc& S, const float* __restrict__ pool,
+                                           float nm1, int q) {
+    if (q < R.lo || q >= R.hi) return make_float2(0.0f, 0.0f);
+    const float m = bin_weight(R, S.mother, pool, nm1, q) * R.out_scale;
+    const float2 xv = __ldg(S.X + q);
+    return make_float2(xv.x * m, xv.y * m);
+}
+
 template <int OT>
 __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
     if constexpr (OT == OUT_C64) {
@@ -156,32 +184,31 @@ __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
     }
 }
 
+// w_N^e with e < N from the SMEM low table and the global high table.
+__device__ __forceinline__ float2 tw_n(const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                                      unsigned e) {
+    return cmul(twlo[e & 1023u], __ldg(twhi + (e >> 10)));
+}
+
 // Phase 1 of one chunk of kChunk k2 values of a row (see fcwt_internal.h):
-// loads Z = Ihat * W into the tile zs[k1][k2], then every (k2, v) task runs a
-// K-point DFT and writes G[c][k2] (c = v + R u) with its twiddle.
+// loads Z into the tile zs[k1][k2], then every (k2, v) task runs a K-point
+// DFT and writes G[c][k2] (c = v + R u) times w_N^{(k2+L) c}.
 template <int K, bool TO_GLOBAL>
-__device__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
+__device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
                              float2* __restrict__ zs, const float2* __restrict__ twlo,
                              float2* __restrict__ gdst) {
     const int tid = threadIdx.x;
     const int log2N = S.log2N;
     const int N = 1 << log2N;
+    const unsigned Nm = (unsigned)N - 1u;
     const int M = N >> kLog2P2;
     const int Rr = M / K;
     const float nm1 = (float)N - 1.0f;
-    const float2* __restrict__ X = S.X;
     // (a) input tile
     for (int idx = tid; idx < K * kChunk; idx += kThreads) {
         const int k1 = idx / kChunk;
         const int kl = idx - k1 * kChunk;
-        const int q = R.L + k2_0 + kl + kP2 * k1;
-        float2 z = make_float2(0.0f, 0.0f);
-        if (q >= R.lo && q < R.hi) {
-            float m = bin_weight(R, S.mother, pool, nm1, q);
-            float2 xv = __ldg(X + q);
-            z = make_float2(xv.x * m, xv.y * m);
-        }
-        zs[idx] = z;
+        zs[idx] = bin_value(R, S, pool, nm1, R.L + k2_0 + kl + kP2 * k1);
     }
     __syncthreads();
     // (b) tasks
@@ -193,22 +220,34 @@ __device__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __
 #pragma unroll
         for (int k1 = 0; k1 < K; k1++) z[k1] = zs[k1 * kChunk + kl];
         if (v != 0) {
+            // pre-twiddle w_M^{v k1}: exact table value every 8 steps, a
+            // running product (at most 7 multiplies) in between
+            const float2 step = __ldg(twhi + v);
+            float2 w = make_float2(1.0f, 0.0f);
 #pragma unroll
-            for (int k1 = 1; k1 < K; k1++) z[k1] = cmul(z[k1], __ldg(twhi + v * k1));
+            for (int k1 = 1; k1 < K; k1++) {
+                w = (k1 & 7) ? cmul(w, step) : __ldg(twhi + v * k1);
+                z[k1] = cmul(z[k1], w);
+            }
         }
         fft_reg<K, +1>(z);
-        const unsigned k2L = (unsigned)(k2_0 + kl + R.L);
         const int k2 = k2_0 + kl;
+        const unsigned k2L = (unsigned)(k2 + R.L);
+        const unsigned base = (k2L * (unsigned)v) & Nm;   // exponent of u = 0
+        const unsigned d = (k2L * (unsigned)Rr) & Nm;     // exponent step per u
+        float2* __restrict__ dst = gdst + k2;
+        // post-twiddle w_N^{base + d u}: exact every 8 outputs, running
+        // product in between
+        const float2 wd = tw_n(twlo, twhi, d);
+        float2 w = make_float2(1.0f, 0.0f);
 #pragma unroll
         for (int u = 0; u < K; u++) {
-            const int c = v + Rr * u;
-            const unsigned e = (k2L * (unsigned)c) & (unsigned)(N - 1);
-            const float2 w = cmul(twlo[e & 1023u], __ldg(twhi + (e >> 10)));
+            w = (u & 7) ? cmul(w, wd) : tw_n(twlo, twhi, (base + (unsigned)u * d) & Nm);
             const float2 g = cmul(z[u], w);
             if constexpr (TO_GLOBAL)
-                __stcg(gdst + (size_t)c * kP2 + k2, g);
+                __stcg(dst + (size_t)(v + Rr * u) * kP2, g);
             else
-                gdst[c * kP2 + k2] = g;
+                dst[(v + Rr * u) * kP2] = g;
         }
     }
     __syncthreads();
@@ -243,8 +282,36 @@ __device__ __forceinline__ void dft1024_warp(float2 (&x)[32], int lane, float2* 
     fft_reg<32, +1>(x);
 }
 
+// Phase 2 of columns [c0, c0 + 8) of a row: one warp per column runs the
+// 1024-point DFT, the outputs y[c0 + w + M a] are staged in SMEM and written as
+// runs of 8 consecutive samples.
 template <int OT>
-__global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
+__device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0, int M, int n, void* outb,
+                                         long long out_off, float2* __restrict__ region0,
+                                         const float2* __restrict__ t2) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const float2* __restrict__ col = G + (size_t)(c0 + warp) * kP2 + lane;
+    float2 x[32];
+#pragma unroll
+    for (int m = 0; m < 32; m++) x[m] = __ldcg(col + 32 * m);
+    dft1024_warp(x, lane, region0 + warp * (32 * 33), t2);
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * kStagePitch + warp] = x[h];
+    __syncthreads();
+    const long long row0 = out_off + c0;
+    for (int idx = tid; idx < kGroupCols * kP2; idx += kThreads) {
+        const int w = idx & (kGroupCols - 1);
+        const int a = idx >> 3;
+        if (c0 + w + M * a < n) store_out<OT>(outb, row0 + w + (long long)M * a, region0[a * kStagePitch + w]);
+    }
+    __syncthreads();
+}
+
+template <int OT>
+__global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
     extern __shared__ float2 smem[];
     float2* region0 = smem;
     float2* zs = smem + kRegion0;
@@ -253,6 +320,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
     __shared__ int s_item;
     __shared__ int s_log2N;
     __shared__ int s_ok;
+    __shared__ RowDesc s_row;
+    __shared__ SigDesc s_sig;
+    __shared__ Item s_it;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -271,13 +341,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
     unsigned* b_done = P.counters + 1 + P.n_rows;
 
     for (;;) {
-        if (tid == 0) s_item = (int)atomicAdd(P.counters, 1u);
+        if (tid == 0) {
+            const int i = (int)atomicAdd(P.counters, 1u);
+            s_item = i;
+            if (i < P.n_items) {
+                s_it = P.items[i];
+                s_row = P.rows[s_it.row];
+                s_sig = P.sigs[s_row.sig];
+            }
+        }
         __syncthreads();
-        const int it = s_item;
-        if (it >= P.n_items) break;
-        const Item item = P.items[it];
-        const RowDesc R = P.rows[item.row];
-        const SigDesc S = P.sigs[R.sig];
+        if (s_item >= P.n_items) break;
+        const Item& item = s_it;
+        const RowDesc& R = s_row;
+        const SigDesc& S = s_sig;
         const int log2N = S.log2N;
         const int N = 1 << log2N;
         const int n = S.n;
@@ -294,11 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
             // N < 1024: direct DFT over the row's nonzero bins.
             const int lo = R.lo, hi = R.hi;
             const float nm1 = (float)N - 1.0f;
-            for (int q = lo + tid; q < hi; q += kThreads) {
-                float m = bin_weight(R, S.mother, P.stale_pool, nm1, q);
-                float2 xv = __ldg(S.X + q);
-                zs[q - lo] = make_float2(xv.x * m, xv.y * m);
-            }
+            for (int q = lo + tid; q < hi; q += kThreads) zs[q - lo] = bin_value(R, S, P.stale_pool, nm1, q);
             __syncthreads();
             for (int t = tid; t < n; t += kThreads) {
                 float2 acc = make_float2(0.0f, 0.0f);
@@ -308,10 +381,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
                     acc.x += z.x * w.x - z.y * w.y;
                     acc.y += z.x * w.y + z.y * w.x;
                 }
-                store_out<OT>(outb, R.out_off + t, cscale(acc, R.out_scale));
+                store_out<OT>(outb, R.out_off + t, acc);
             }
         } else if (item.type == ITEM_FUSED) {
-            // whole row in this CTA: phase 1 into SMEM, then phase 2
+            // whole row in this CTA (N <= 8192, M <= 8 columns): phase 1 into
+            // SMEM, then one warp per column
             const int M = N >> kLog2P2;
             for (int k2_0 = 0; k2_0 < kP2; k2_0 += kChunk)
                 phase1_chunk_dispatch<false>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, region0);
@@ -325,14 +399,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
             __syncthreads();
             if (warp < M) {
 #pragma unroll
-                for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * 17 + warp] = x[h];
+                for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * kStagePitch + warp] = x[h];
             }
             __syncthreads();
             const int log2M = log2N - kLog2P2;
             for (int t = tid; t < n; t += kThreads) {
                 const int c = t & (M - 1);
                 const int a = t >> log2M;
-                store_out<OT>(outb, R.out_off + t, cscale(region0[a * 17 + c], R.out_scale));
+                store_out<OT>(outb, R.out_off + t, region0[a * kStagePitch + c]);
             }
         } else if (item.type == ITEM_PHASE1) {
             if (tid == 0) {
@@ -343,8 +417,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
             __syncthreads();
             if (s_ok) {
                 float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
-                const int k2_0 = item.part * kChunk;
-                phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, G);
+                phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, item.part * kChunk, zs, twlo, G);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(a_done + item.row, 1u);
@@ -354,25 +427,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_row_engine(EngineParams P) {
             if (tid == 0) s_ok = wait_counter(a_done + item.row, (unsigned)R.n_a, P.err) ? 1 : 0;
             __syncthreads();
             if (s_ok) {
-                const int M = N >> kLog2P2;
                 const float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
-                const int c0 = item.part * kGroupCols;
-                const int c = c0 + warp;
-                float2 x[32];
-#pragma unroll
-                for (int m = 0; m < 32; m++) x[m] = __ldcg(G + (size_t)c * kP2 + lane + 32 * m);
-                dft1024_warp(x, lane, region0 + warp * (32 * 33), t2);
-                __syncthreads();
-#pragma unroll
-                for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * 17 + warp] = x[h];
-                __syncthreads();
-                for (int idx = tid; idx < kGroupCols * kP2; idx += kThreads) {
-                    const int w = idx & (kGroupCols - 1);
-                    const int a = idx >> 4;
-                    const long long t = (long long)c0 + w + (long long)M * a;
-                    if (t < n) store_out<OT>(outb, R.out_off + t, cscale(region0[a * 17 + w], R.out_scale));
-                }
-                __syncthreads();
+                phase2_item<OT>(G, item.part * kGroupCols, N >> kLog2P2, n, outb, R.out_off, region0, t2);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(b_done + item.row, 1u);
@@ -474,6 +530,12 @@ cudaError_t engine_configure() {
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(dev::k_row_engine<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dev::kEngineSmemBytes);
+}
+
+// Resident CTAs of the row engine per SM (the persistent grid is SMs x this).
+cudaError_t engine_blocks_per_sm(int* out) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, dev::k_row_engine<OUT_C64>, kThreads,
+                                                         dev::kEngineSmemBytes);
 }
 
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st) {

@@ -14,8 +14,9 @@ constexpr unsigned kFlagExactSupport = 1u << 2;
 
 // Relative weight below which a bin's daughter value is skipped (unless
 // kFlagExactSupport): mother[w] < kTrimRel * max(mother). The skipped terms
-// change each output by at most kTrimRel * max|W| * sum|Ihat| / N.
-constexpr double kTrimRel = 5.684341886080802e-14;  // 2^-44
+// change each output by at most kTrimRel * max|W| * sum|Ihat| / N, i.e.
+// 1.5e-11 of the largest weight: far below float32 resolution.
+constexpr double kTrimRel = 1.4551915228366852e-11;  // 2^-36
 
 struct RowPlan {
     int proc = 0;     // own truncation length

@@ -40,7 +40,7 @@ extern "C" {
 /* ---- transform flags */
 #define FCWT_NORM (1u << 0)           /* divide by N: FCWT(..., use_normalization=true) */
 #define FCWT_SCALAR_TRUNC (1u << 1)   /* truncation rule of the reference's non-AVX build */
-#define FCWT_EXACT_SUPPORT (1u << 2)  /* also evaluate bins whose weight is < 2^-44 of the peak */
+#define FCWT_EXACT_SUPPORT (1u << 2)  /* also evaluate bins whose weight is < 2^-36 of the peak */
 
 /* ---- output element types */
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
@@ -57,7 +57,8 @@ const char* fcwt_last_error(void);
  * Calls on one context are not reentrant. */
 int fcwt_context_create(int device, fcwt_context** ctx);
 int fcwt_context_destroy(fcwt_context* ctx);
-/* Use an external cudaStream_t (passed as void*); NULL restores the own stream. */
+/* Use an external cudaStream_t (passed as void*); NULL restores the context's
+ * own stream. Pass (void*)1 (cudaStreamLegacy) for the legacy default stream. */
 int fcwt_context_set_stream(fcwt_context* ctx, void* cuda_stream);
 /* Wait for all work of the context and report device-side errors. */
 int fcwt_synchronize(fcwt_context* ctx);

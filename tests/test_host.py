@@ -128,7 +128,7 @@ def test_context_creation_fails_cleanly_without_gpu():
 
 @pytest.mark.parametrize("fb,case", [(2.0, 0), (0.5, 0), (6.0, 4), (2.0, 1)])
 def test_bin_window_drops_only_negligible_weights(oracle, fcwt, golden, fb, case):
-    """Bins outside the planner's [lo, hi) window carry weight below 2^-44 of
+    """Bins outside the planner's [lo, hi) window carry weight below 2^-36 of
     the mother peak (the trimming bound), for own and stale bins alike."""
     st, fs, f0, f1, fn = golden["scale_cases"][case]
     sc = golden[f"scales_{case}"][:: max(1, int(fn) // 60)].copy()
@@ -142,7 +142,7 @@ def test_bin_window_drops_only_negligible_weights(oracle, fcwt, golden, fb, case
             mask = np.ones(N // 2, bool)
             mask[lo[i]:hi[i]] = False
             if mask.any():
-                assert W[i][mask].max(initial=0.0) < 2.0 ** -44 * peak * (1 + 1e-6), (i, T)
+                assert W[i][mask].max(initial=0.0) < 2.0 ** -36 * peak * (1 + 1e-6), (i, T)
         # exact mode keeps every nonzero bin
         _, lo_e, hi_e = fcwt.row_truncation(n, sc, T, exact_support=True, fb=fb)
         for i in range(sc.size):
