@@ -58,6 +58,7 @@ SIGNATURES = {
     "fcwt_plan_destroy": (_i, [_vp]),
     "fcwt_create_optimization_plan": (_i, [_vp, _i, _i, _i, ctypes.c_char_p]),
     "fcwt_load_optimization_plan": (_i, [_vp, _i, _i, ctypes.c_char_p]),
+    "fcwt_cwt_noalloc": (_i, [_vp, _i, _f, _vp, _i, _i, _u, _vp, _vp, ctypes.POINTER(_i)]),
 }
 
 

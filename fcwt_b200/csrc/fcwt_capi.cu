@@ -398,6 +398,12 @@ std::string tune_path(const char* dir, int N, int threads) {
 
 }  // namespace
 
+namespace fcwt {
+// Lets other translation units of the library set the message that
+// fcwt_last_error() returns for the calling thread.
+void record_error(const std::string& msg) { g_err = msg; }
+}  // namespace fcwt
+
 // =================================================================== C ABI
 
 extern "C" {

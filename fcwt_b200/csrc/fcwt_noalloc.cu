@@ -1,0 +1,263 @@
+// fcwt_cwt_noalloc: the real-input transform for callers that cannot allocate
+// device memory.
+//
+// Who needs it: code that runs on a real-time thread (an audio or sensor
+// callback that must not block), where cudaMalloc/cudaFree can stall and
+// implicitly synchronize the device; plug-ins hosted by a framework that owns
+// all device memory; and callers that fix their memory footprint at start-up.
+//
+// Everything the call needs on the device besides the caller's input and
+// output lives in one file-scope __device__ array of kNoAllocScratchBytes
+// (about 2.3 MB, held by every GPU that loads the library until the process
+// exits): the spectrum, the FFT ping-pong buffer, the mother and twiddle
+// tables, the stale-bin tables, the row and work-item descriptors, the work
+// queue counters and the scratch ring of the two-phase rows. Its limits:
+// n <= 16384 samples, fn <= 1024 scales, at most 8 distinct stale-bin tables.
+//
+// Every call shares that array and leaves its contents behind; each call
+// clears the counters and error word it needs before its kernels run. Calls
+// whose GPU work overlaps (different streams, or different host threads on
+// one device) race on the array: serialize them on one stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fcwt_b200.h"
+#include "fcwt_internal.h"
+#include "fcwt_plan.h"
+
+namespace fcwt {
+cudaError_t launch_mother(float fb, int N, float norm, float* out, cudaStream_t st);
+cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st);
+cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
+                           float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
+cudaError_t engine_configure();
+cudaError_t engine_blocks_per_sm(int* out);
+cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
+void record_error(const std::string& msg);  // message returned by fcwt_last_error()
+}  // namespace fcwt
+
+namespace {
+
+using namespace fcwt;
+
+constexpr int kNaMaxN = 16384;
+constexpr int kNaMaxRows = 1024;
+constexpr int kNaMaxTables = 8;
+constexpr int kNaSlots = 8;
+constexpr int kNaMaxItems = kNaMaxRows * (kP2 / kChunk + kNaMaxN / kP2 / kGroupCols);
+
+// byte offsets of the sub-buffers inside the array (256-byte aligned)
+constexpr size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+constexpr size_t kOffX = 0;
+constexpr size_t kOffTmp = align256(kOffX + sizeof(float2) * kNaMaxN);
+constexpr size_t kOffMother = align256(kOffTmp + sizeof(float2) * kNaMaxN);
+constexpr size_t kOffTw = align256(kOffMother + sizeof(float) * kNaMaxN);
+constexpr size_t kOffPool = align256(kOffTw + sizeof(float2) * (kP2 + kNaMaxN / kP2));
+constexpr size_t kOffRows = align256(kOffPool + sizeof(float) * kNaMaxTables * (kNaMaxN / 2));
+constexpr size_t kOffItems = align256(kOffRows + sizeof(RowDesc) * kNaMaxRows);
+constexpr size_t kOffSig = align256(kOffItems + sizeof(Item) * kNaMaxItems);
+constexpr size_t kOffCounters = align256(kOffSig + sizeof(SigDesc));
+constexpr size_t kOffErr = align256(kOffCounters + sizeof(unsigned) * (1 + 2 * kNaMaxRows));
+constexpr size_t kOffScratch = align256(kOffErr + sizeof(int));
+constexpr size_t kNoAllocScratchBytes = align256(kOffScratch + sizeof(float2) * kNaSlots * kNaMaxN);
+
+// The array itself. Host code must not use its name as an address: on the
+// host it is only a stand-in symbol; the device address comes from
+// cudaGetSymbolAddress during the per-device set-up below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+int na_fail(int code, const std::string& msg) {
+    record_error(msg);
+    return code;
+}
+
+struct DeviceSetup {
+    bool ready = false;
+    unsigned char* base = nullptr;  // device address of g_noalloc_scratch on that device
+    int grid = 0;                   // persistent grid of the row engine
+};
+
+std::mutex g_setup_mu;
+DeviceSetup g_setup[64];
+
+// Once per device, with that device current: resolve the array's device
+// address and configure the row engine.
+int setup_device(int dev, DeviceSetup** out) {
+    if (dev < 0 || dev >= 64) return na_fail(FCWT_ERR_UNSUPPORTED, "device index >= 64");
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    DeviceSetup& s = g_setup[dev];
+    if (!s.ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return na_fail(FCWT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        e = engine_configure();
+        if (e != cudaSuccess) return na_fail(FCWT_ERR_CUDA, std::string("engine set-up: ") + cudaGetErrorString(e));
+        int per_sm = 0, sms = 0;
+        e = engine_blocks_per_sm(&per_sm);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return na_fail(FCWT_ERR_CUDA, std::string("engine set-up: ") + cudaGetErrorString(e));
+        s.base = static_cast<unsigned char*>(p);
+        s.grid = std::max(1, per_sm) * sms;
+        s.ready = true;
+    }
+    *out = &s;
+    return FCWT_OK;
+}
+
+bool on_device(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+#define NA_TRY(expr)                                                                          \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess) return na_fail(FCWT_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float* scales, int fn, int threads,
+                                unsigned flags, void* output, void* stream, int* status) {
+    if (n < 0 || fn < 0) return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: negative size");
+    if (n > kNaMaxN)
+        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: n = " + std::to_string(n) +
+                                             " exceeds the static scratch limit of 16384 samples");
+    if (fn > kNaMaxRows)
+        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: fn = " + std::to_string(fn) +
+                                             " exceeds the static scratch limit of 1024 scales");
+    if (status) *status = 0;
+    if (n == 0 || fn == 0) return FCWT_OK;
+    if (!input || !output || !scales) return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: null pointer");
+    if (!on_device(input) || !on_device(output))
+        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: input and output must be device pointers");
+    int dev = 0;
+    NA_TRY(cudaGetDevice(&dev));
+    DeviceSetup* S = nullptr;
+    int rc = setup_device(dev, &S);
+    if (rc) return rc;
+
+    SignalPlan sp;
+    std::string err;
+    if (plan_signal(n, false, fb, scales, fn, threads, flags, sp, err)) return na_fail(FCWT_ERR_INVALID, err);
+    if ((int)sp.tables.size() > kNaMaxTables)
+        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: the scale sequence needs more than 8 stale-bin tables");
+    const int N = sp.N;
+    const int M = sp.M;
+    for (const RowPlan& rp : sp.rows)
+        if (N >= kP2 && rp.K > kMaxK) return na_fail(FCWT_ERR_UNSUPPORTED, "fcwt_cwt_noalloc: row support too wide");
+
+    // descriptors (same work list as a plan of the row engine)
+    std::vector<RowDesc> rows((size_t)fn);
+    std::vector<Item> items;
+    std::vector<float> pool;
+    for (const auto& T : sp.tables) pool.insert(pool.end(), T.begin(), T.end());
+    const float out_scale = (flags & kFlagNorm) ? 1.0f / (float)N : 1.0f;
+    const bool two_phase = N > kMaxFusedN;
+    int S_slots = 0;
+    for (int r = 0; r < fn; r++) {
+        const RowPlan& rp = sp.rows[(size_t)r];
+        RowDesc& d = rows[(size_t)r];
+        std::memset(&d, 0, sizeof(d));
+        d.sig = 0;
+        d.proc = rp.proc;
+        d.step = rp.step;
+        d.K = rp.K;
+        d.L = rp.L;
+        d.lo = rp.lo;
+        d.hi = rp.hi;
+        d.stale = rp.table >= 0 ? rp.table * sp.half : -1;
+        d.slot = -1;
+        d.wait_row = -1;
+        d.out_buf = 0;
+        d.out_off = (long long)r * n;
+        d.out_scale = out_scale;
+    }
+    if (!two_phase) {
+        const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;
+        for (int r = 0; r < fn; r++) items.push_back({type, r, 0, 0});
+    } else {
+        S_slots = std::min(kNaSlots, fn);
+        const int D = std::max(1, std::min(12, S_slots / 2));
+        const int n_a = kP2 / kChunk;
+        const int n_b = M / kGroupCols;
+        for (int r = 0; r < fn; r++) {
+            rows[(size_t)r].slot = r % S_slots;
+            rows[(size_t)r].wait_row = r >= S_slots ? r - S_slots : -1;
+            rows[(size_t)r].n_a = n_a;
+            rows[(size_t)r].n_b = n_b;
+        }
+        for (int step = 0; step < fn + D; step++) {
+            if (step < fn)
+                for (int a = 0; a < n_a; a++) items.push_back({ITEM_PHASE1, step, a, 0});
+            const int rb = step - D;
+            if (rb >= 0 && rb < fn)
+                for (int b = 0; b < n_b; b++) items.push_back({ITEM_PHASE2, rb, b, 0});
+        }
+    }
+
+    unsigned char* base = S->base;
+    float2* X = reinterpret_cast<float2*>(base + kOffX);
+    float2* tmp = reinterpret_cast<float2*>(base + kOffTmp);
+    float* mother = reinterpret_cast<float*>(base + kOffMother);
+    float2* tw = reinterpret_cast<float2*>(base + kOffTw);
+    float* dpool = reinterpret_cast<float*>(base + kOffPool);
+    RowDesc* drows = reinterpret_cast<RowDesc*>(base + kOffRows);
+    Item* ditems = reinterpret_cast<Item*>(base + kOffItems);
+    SigDesc* dsig = reinterpret_cast<SigDesc*>(base + kOffSig);
+    unsigned* counters = reinterpret_cast<unsigned*>(base + kOffCounters);
+    int* derr = reinterpret_cast<int*>(base + kOffErr);
+    float2* scratch = reinterpret_cast<float2*>(base + kOffScratch);
+
+    cudaStream_t st = (cudaStream_t)stream;
+    SigDesc sd;
+    sd.X = X;
+    sd.mother = mother;
+    sd.tw = tw;
+    sd.log2N = sp.log2N;
+    sd.n = n;
+    NA_TRY(cudaMemcpyAsync(dsig, &sd, sizeof(sd), cudaMemcpyHostToDevice, st));
+    NA_TRY(cudaMemcpyAsync(drows, rows.data(), rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
+    NA_TRY(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice, st));
+    if (!pool.empty())
+        NA_TRY(cudaMemcpyAsync(dpool, pool.data(), pool.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    NA_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)fn), st));
+    NA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), st));
+    NA_TRY(launch_mother(fb, N, host::mother_norm(), mother, st));
+    NA_TRY(launch_twiddle(sp.log2N, tw, st));
+    int n_fwd = 0;
+    NA_TRY(launch_forward(input, nullptr, n, sp.log2N, tw, X, tmp, st, &n_fwd));
+    EngineParams ep;
+    std::memset(&ep, 0, sizeof(ep));
+    ep.sigs = dsig;
+    ep.rows = drows;
+    ep.items = ditems;
+    ep.n_items = (int)items.size();
+    ep.stale_pool = dpool;
+    ep.scratch = two_phase ? scratch : nullptr;
+    ep.slot_elems = two_phase ? N : 0;
+    ep.counters = counters;
+    ep.n_rows = fn;
+    ep.outs[0] = output;
+    ep.out_type = OUT_C64;
+    ep.err = derr;
+    NA_TRY(launch_engine(ep, std::max(1, std::min(ep.n_items, S->grid)), st));
+    if (status) {
+        int h = 0;
+        NA_TRY(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        NA_TRY(cudaStreamSynchronize(st));
+        *status = h;
+        if (h != 0) return na_fail(FCWT_ERR_DEVICE, "fcwt_cwt_noalloc: row engine reported error bits " + std::to_string(h));
+    }
+    return FCWT_OK;
+}

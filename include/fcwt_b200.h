@@ -131,6 +131,25 @@ int fcwt_create_optimization_plan(fcwt_context* ctx, int maxsize, int threads, i
  * keeps its defaults). */
 int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const char* directory);
 
+/* ---- allocation-free transform
+ * No counterpart in the reference. Same result as fcwt_cwt (real input,
+ * complex64 output) for callers that cannot allocate device memory: code on a
+ * real-time thread (audio/sensor callbacks) where cudaMalloc may block and
+ * synchronize the device, plug-ins whose host framework owns all device
+ * memory, and callers that fix their footprint at start-up. The call
+ * allocates nothing: all its device workspace is one static array of about
+ * 2.3 MB inside the library (held on every GPU that loads the library).
+ * Limits: n <= 16384, fn <= 1024, at most 8 stale-bin tables; larger
+ * requests fail with FCWT_ERR_INVALID. input/output must be device pointers;
+ * scales is a host array; work is enqueued on `stream` (a cudaStream_t, NULL
+ * = legacy default stream). The first call on a device resolves the array's
+ * address and configures the kernels for that device: make it before any
+ * stream capture. All calls share the array: calls whose GPU work overlaps
+ * race; serialize them on one stream. With status != NULL the call waits for
+ * its work and stores the device error word there (0 = ok). */
+int fcwt_cwt_noalloc(const float* input, int n, float fb, const float* scales, int fn, int threads,
+                     unsigned flags, void* output, void* stream, int* status);
+
 #ifdef __cplusplus
 }
 #endif
