@@ -1,5 +1,7 @@
 // C ABI of the B200 fCWT path: contexts, plans, transforms and tuning files.
 // See include/fcwt_b200.h for the contract of each entry point.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +27,7 @@ cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log
 cudaError_t engine_configure();
 cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
+cudaError_t launch_engine(const EngineParams& p, const CUtensorMap& omap, int grid, cudaStream_t st);
 }  // namespace fcwt
 
 namespace {
@@ -88,6 +91,40 @@ bool is_device_pointer(const void* p) {
 }
 
 size_t out_elem_bytes(int out_type) { return out_type == FCWT_OUT_C64 ? 8 : 4; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map of a complex64 [rows][n] output seen as [rows][n / M][M]
+// (8-byte elements), boxes of [1][256][8], 64B swizzle. Only complete
+// stripes a < n / M are covered. Requires n even and a 16-byte aligned base.
+bool encode_output_map(void* base, int n, int M, int rows, CUtensorMap* map) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (n & 1) || ((uintptr_t)base & 15) || n / M < 1 || rows < 1) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)M, (cuuint64_t)(n / M), (cuuint64_t)rows};
+    cuuint64_t strides[2] = {(cuuint64_t)M * 8, (cuuint64_t)n * 8};
+    cuuint32_t box[3] = {8, 256, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -185,7 +222,7 @@ int plan_build(fcwt_plan* P) {
         d.out_buf = 0;
         d.out_off = (long long)r * sp.n;
         d.out_scale = out_scale;
-        d.pad = 0;
+        d.out_row = r;
         if (N >= kP2 && rp.K > kMaxK)
             return fail(FCWT_ERR_UNSUPPORTED,
                         "row support wider than 32768 bins at N > 16384 is not implemented in this build");
@@ -310,6 +347,10 @@ int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
     ep.outs[0] = dout;
     ep.out_type = out_type;
     ep.err = ctx->err.as<int>();
+    CUtensorMap omap;
+    std::memset(&omap, 0, sizeof(omap));
+    ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64 &&
+                    encode_output_map(dout, n, sp.M, P->n_rows, &omap)) ? 1 : 0;
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (ctx->profiling) {
@@ -322,7 +363,7 @@ int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
         }
         FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
     }
-    FCWT_CUDA_TRY(launch_engine(ep, grid, st));
+    FCWT_CUDA_TRY(launch_engine(ep, omap, grid, st));
     ctx->kernel_launches += 1;
     if (ctx->profiling) {
         FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));

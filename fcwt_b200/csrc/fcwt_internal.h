@@ -60,7 +60,7 @@ struct RowDesc {
     int out_buf;      // index of the output buffer
     long long out_off;  // element offset of the row inside that buffer
     float out_scale;  // 1/N or 1
-    int pad;
+    int out_row;      // row index inside that buffer (for tensor-map stores)
 };
 
 enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3 };
@@ -88,6 +88,7 @@ struct EngineParams {
     void* outs[kMaxOuts];      // output buffers (passed by value with the launch)
     int out_type;
     int* err;                  // device error word (0 = ok)
+    int tma_store;             // phase-2 outputs via the tensor map (buffer 0, complex64, even n)
 };
 
 // Error bits written by device code into EngineParams::err.

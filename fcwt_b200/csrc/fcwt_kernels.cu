@@ -13,10 +13,12 @@
 //                 inverse FFT (fcwt.cpp:418-429), normalisation
 //                 (fcwt.cpp:431-445) and crop to n (fcwt.cpp:396-416), fused,
 //                 driven by a work queue of per-row items.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "fcwt_fft.cuh"
 #include "fcwt_internal.h"
@@ -103,11 +105,19 @@ __global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restr
 //   zs:      phase-1 input tile [K][kChunk]
 //   twlo:    w_N^j, j < 1024, of the current N
 //   t2:      w_1024^{a l} at [a*32 + l]
+//   twhi:    w_N^{1024 j}, j < M, of the current N (when M <= 512)
 constexpr int kStagePitch = kGroupCols + 1;
 constexpr int kRegion0 = kP2 * kStagePitch;
 constexpr int kZs = kChunk * kMaxK;
-constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 + kP2;
-constexpr size_t kEngineSmemBytes = (size_t)kSmemFloat2 * sizeof(float2);
+constexpr int kTwhiSmem = 512;
+constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 + kP2 + kTwhiSmem;
+constexpr size_t kSmemAlign = 1024;  // the 64B-swizzled staging tile wants 1 KB alignment
+constexpr size_t kEngineSmemBytes = (size_t)kSmemFloat2 * sizeof(float2) + kSmemAlign;
+// Phase-2 staging for tensor-map stores: 4 boxes of [256 a][8 columns] complex64.
+constexpr int kBoxRows = 256;
+constexpr int kBoxBytes = kBoxRows * kGroupCols * 8;
+static_assert(4 * kBoxBytes <= kRegion0 * 8, "staging boxes fit in region0");
+constexpr int kFetchBatch = 2;  // work items claimed per queue access
 static_assert(kRegion0 >= kMaxFusedN, "fused rows keep G in region0");
 static_assert(kRegion0 >= (kThreads / 32) * 32 * 33, "per-warp transposes live in region0");
 
@@ -184,10 +194,31 @@ __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
     }
 }
 
-// w_N^e with e < N from the SMEM low table and the global high table.
+// ---- bulk-async (TMA) store helpers
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* smem, int c0, int c1, int c2) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(reinterpret_cast<unsigned long long>(map)), "r"(s), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Byte offset of staging element (a, w) in the 64B-swizzled box layout the
+// tensor map expects: 16-byte chunk bits [4:5] XOR address bits [7:8].
+__device__ __forceinline__ unsigned stage_off(int a, int w) {
+    const unsigned lin = (unsigned)((a & (kBoxRows - 1)) * (kGroupCols * 8) + w * 8);
+    return (unsigned)(a >> 8) * kBoxBytes + (lin ^ (((lin >> 7) & 3u) << 4));
+}
+
+// w_N^e with e < N from the low table (SMEM) and the high table (SMEM when
+// M <= 1024, else global).
 __device__ __forceinline__ float2 tw_n(const float2* __restrict__ twlo, const float2* __restrict__ twhi,
                                       unsigned e) {
-    return cmul(twlo[e & 1023u], __ldg(twhi + (e >> 10)));
+    return cmul(twlo[e & 1023u], twhi[e >> 10]);
 }
 
 // Phase 1 of one chunk of kChunk k2 values of a row (see fcwt_internal.h):
@@ -196,7 +227,7 @@ __device__ __forceinline__ float2 tw_n(const float2* __restrict__ twlo, const fl
 template <int K, bool TO_GLOBAL>
 __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
                              float2* __restrict__ zs, const float2* __restrict__ twlo,
-                             float2* __restrict__ gdst) {
+                             const float2* __restrict__ twhi, float2* __restrict__ gdst) {
     const int tid = threadIdx.x;
     const int log2N = S.log2N;
     const int N = 1 << log2N;
@@ -212,7 +243,6 @@ __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R,
     }
     __syncthreads();
     // (b) tasks
-    const float2* __restrict__ twhi = S.tw + kP2;
     for (int t = tid; t < kChunk * Rr; t += kThreads) {
         const int kl = t % kChunk;
         const int v = t / kChunk;
@@ -222,11 +252,11 @@ __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R,
         if (v != 0) {
             // pre-twiddle w_M^{v k1}: exact table value every 8 steps, a
             // running product (at most 7 multiplies) in between
-            const float2 step = __ldg(twhi + v);
+            const float2 step = twhi[v];
             float2 w = make_float2(1.0f, 0.0f);
 #pragma unroll
             for (int k1 = 1; k1 < K; k1++) {
-                w = (k1 & 7) ? cmul(w, step) : __ldg(twhi + v * k1);
+                w = (k1 & 7) ? cmul(w, step) : twhi[v * k1];
                 z[k1] = cmul(z[k1], w);
             }
         }
@@ -255,14 +285,15 @@ __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R,
 
 template <bool TO_GLOBAL>
 __device__ void phase1_chunk_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool,
-                                      int k2_0, float2* zs, const float2* twlo, float2* gdst) {
+                                      int k2_0, float2* zs, const float2* twlo, const float2* twhi,
+                                      float2* gdst) {
     switch (K) {
-        case 1: phase1_chunk<1, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
-        case 2: phase1_chunk<2, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
-        case 4: phase1_chunk<4, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
-        case 8: phase1_chunk<8, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
-        case 16: phase1_chunk<16, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
-        default: phase1_chunk<32, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, gdst); break;
+        case 1: phase1_chunk<1, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
+        case 2: phase1_chunk<2, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
+        case 4: phase1_chunk<4, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
+        case 8: phase1_chunk<8, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
+        case 16: phase1_chunk<16, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
+        default: phase1_chunk<32, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
     }
 }
 
@@ -283,12 +314,15 @@ __device__ __forceinline__ void dft1024_warp(float2 (&x)[32], int lane, float2* 
 }
 
 // Phase 2 of columns [c0, c0 + 8) of a row: one warp per column runs the
-// 1024-point DFT, the outputs y[c0 + w + M a] are staged in SMEM and written as
-// runs of 8 consecutive samples.
+// 1024-point DFT; the outputs y[c0 + w + M a] go out either through the tensor
+// map (4 bulk stores of [256 a][8 w] boxes from a swizzled SMEM tile, issued by
+// thread 0 and completed asynchronously; the partial last stripe a = n / M is
+// stored by threads) or, without a tensor map, as runs of 8 samples stored by
+// all threads from a padded SMEM tile.
 template <int OT>
 __device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0, int M, int n, void* outb,
-                                         long long out_off, float2* __restrict__ region0,
-                                         const float2* __restrict__ t2) {
+                                         long long out_off, int out_row, float2* __restrict__ region0,
+                                         const float2* __restrict__ t2, const CUtensorMap* omap, bool tma) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -298,31 +332,55 @@ __device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0
     for (int m = 0; m < 32; m++) x[m] = __ldcg(col + 32 * m);
     dft1024_warp(x, lane, region0 + warp * (32 * 33), t2);
     __syncthreads();
-#pragma unroll
-    for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * kStagePitch + warp] = x[h];
-    __syncthreads();
     const long long row0 = out_off + c0;
-    for (int idx = tid; idx < kGroupCols * kP2; idx += kThreads) {
-        const int w = idx & (kGroupCols - 1);
-        const int a = idx >> 3;
-        if (c0 + w + M * a < n) store_out<OT>(outb, row0 + w + (long long)M * a, region0[a * kStagePitch + w]);
+    if (tma) {
+        unsigned char* stage = reinterpret_cast<unsigned char*>(region0);
+#pragma unroll
+        for (int h = 0; h < 32; h++)
+            *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * h, warp)) = x[h];
+        fence_proxy_async_smem();
+        __syncthreads();
+        const int n_full = n / M;  // stripes a < n_full are complete
+        if (tid == 0) {
+            for (int j = 0; j < 4 && j * kBoxRows < n_full; j++)
+                tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, out_row);
+            bulk_commit();
+        }
+        const int tail = n - n_full * M;  // samples of the partial stripe a = n_full
+        if (tid < kGroupCols && c0 + tid < tail && n_full < kP2)
+            store_out<OT>(outb, row0 + tid + (long long)M * n_full,
+                          *reinterpret_cast<const float2*>(stage + stage_off(n_full, tid)));
+        // region0 is reused only after thread 0 waited for the bulk reads
+    } else {
+#pragma unroll
+        for (int h = 0; h < 32; h++) region0[(lane + 32 * h) * kStagePitch + warp] = x[h];
+        __syncthreads();
+        for (int idx = tid; idx < kGroupCols * kP2; idx += kThreads) {
+            const int w = idx & (kGroupCols - 1);
+            const int a = idx >> 3;
+            if (c0 + w + M * a < n) store_out<OT>(outb, row0 + w + (long long)M * a, region0[a * kStagePitch + w]);
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 template <int OT>
-__global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
-    extern __shared__ float2 smem[];
+__global__ void __launch_bounds__(kThreads, 2)
+    k_row_engine(const __grid_constant__ EngineParams P, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    float2* smem = reinterpret_cast<float2*>(
+        smem_raw + ((kSmemAlign - ((size_t)__cvta_generic_to_shared(smem_raw) & (kSmemAlign - 1))) & (kSmemAlign - 1)));
     float2* region0 = smem;
     float2* zs = smem + kRegion0;
     float2* twlo = zs + kZs;
     float2* t2 = twlo + kP2;
+    float2* twhi_s = t2 + kP2;
     __shared__ int s_item;
     __shared__ int s_log2N;
     __shared__ int s_ok;
-    __shared__ RowDesc s_row;
-    __shared__ SigDesc s_sig;
-    __shared__ Item s_it;
+    __shared__ RowDesc s_rows[kFetchBatch];
+    __shared__ SigDesc s_sigs[kFetchBatch];
+    __shared__ Item s_its[kFetchBatch];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -340,29 +398,44 @@ __global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
     unsigned* a_done = P.counters + 1;
     unsigned* b_done = P.counters + 1 + P.n_rows;
 
+    // Items are claimed kFetchBatch at a time (one atomic and one round of
+    // descriptor loads per batch) and processed in claim order.
     for (;;) {
         if (tid == 0) {
-            const int i = (int)atomicAdd(P.counters, 1u);
+            const int i = (int)atomicAdd(P.counters, (unsigned)kFetchBatch);
             s_item = i;
-            if (i < P.n_items) {
-                s_it = P.items[i];
-                s_row = P.rows[s_it.row];
-                s_sig = P.sigs[s_row.sig];
-            }
+#pragma unroll
+            for (int b = 0; b < kFetchBatch; b++)
+                if (i + b < P.n_items) s_its[b] = P.items[i + b];
+#pragma unroll
+            for (int b = 0; b < kFetchBatch; b++)
+                if (i + b < P.n_items) s_rows[b] = P.rows[s_its[b].row];
+#pragma unroll
+            for (int b = 0; b < kFetchBatch; b++)
+                if (i + b < P.n_items) s_sigs[b] = P.sigs[s_rows[b].sig];
         }
         __syncthreads();
         if (s_item >= P.n_items) break;
-        const Item& item = s_it;
-        const RowDesc& R = s_row;
-        const SigDesc& S = s_sig;
+      for (int bi = 0; bi < kFetchBatch && s_item + bi < P.n_items; bi++) {
+        const Item& item = s_its[bi];
+        const RowDesc& R = s_rows[bi];
+        const SigDesc& S = s_sigs[bi];
         const int log2N = S.log2N;
         const int N = 1 << log2N;
         const int n = S.n;
         void* outb = P.outs[R.out_buf];
+        const int Mcols = N >> kLog2P2;
+        const float2* twhi = (Mcols <= kTwhiSmem) ? twhi_s : S.tw + kP2;
 
-        // twiddle table of this N into SMEM (first 1024 entries)
+        // region0 may still be read by the bulk stores of the previous phase-2 item
+        if (P.tma_store && (item.type == ITEM_PHASE2 || item.type == ITEM_FUSED)) {
+            if (tid == 0) bulk_wait_read_all();
+            __syncthreads();
+        }
+        // twiddle tables of this N into SMEM
         if (s_log2N != log2N) {
             for (int j = tid; j < kP2; j += kThreads) twlo[j] = S.tw[j];
+            for (int j = tid; j < Mcols && Mcols <= kTwhiSmem; j += kThreads) twhi_s[j] = S.tw[kP2 + j];
             __syncthreads();
             if (tid == 0) s_log2N = log2N;
         }
@@ -388,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
             // SMEM, then one warp per column
             const int M = N >> kLog2P2;
             for (int k2_0 = 0; k2_0 < kP2; k2_0 += kChunk)
-                phase1_chunk_dispatch<false>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, region0);
+                phase1_chunk_dispatch<false>(R.K, S, R, P.stale_pool, k2_0, zs, twlo, twhi, region0);
             float2 x[32];
             if (warp < M) {
 #pragma unroll
@@ -417,7 +490,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
             __syncthreads();
             if (s_ok) {
                 float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
-                phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, item.part * kChunk, zs, twlo, G);
+                phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, item.part * kChunk, zs, twlo, twhi, G);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(a_done + item.row, 1u);
@@ -428,7 +501,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
             __syncthreads();
             if (s_ok) {
                 const float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
-                phase2_item<OT>(G, item.part * kGroupCols, N >> kLog2P2, n, outb, R.out_off, region0, t2);
+                phase2_item<OT>(G, item.part * kGroupCols, N >> kLog2P2, n, outb, R.out_off, R.out_row, region0, t2,
+                                &omap, P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(b_done + item.row, 1u);
@@ -438,7 +512,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_row_engine(EngineParams P) {
             if (tid == 0) atomicOr(P.err, kErrBadItem);
         }
         __syncthreads();
+      }
     }
+    if (tid == 0 && P.tma_store) bulk_wait_all();
 }
 
 }  // namespace dev
@@ -538,13 +614,21 @@ cudaError_t engine_blocks_per_sm(int* out) {
                                                          dev::kEngineSmemBytes);
 }
 
-cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st) {
+cudaError_t launch_engine(const EngineParams& p, const CUtensorMap& omap, int grid, cudaStream_t st) {
     switch (p.out_type) {
-        case OUT_BF16: dev::k_row_engine<OUT_BF16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
-        case OUT_F16: dev::k_row_engine<OUT_F16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
-        default: dev::k_row_engine<OUT_C64><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p); break;
+        case OUT_BF16: dev::k_row_engine<OUT_BF16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
+        case OUT_F16: dev::k_row_engine<OUT_F16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
+        default: dev::k_row_engine<OUT_C64><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st) {
+    CUtensorMap none;
+    memset(&none, 0, sizeof(none));
+    EngineParams q = p;
+    q.tma_store = 0;
+    return launch_engine(q, none, grid, st);
 }
 
 }  // namespace fcwt

@@ -182,6 +182,7 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
         d.out_buf = 0;
         d.out_off = (long long)r * n;
         d.out_scale = out_scale;
+        d.out_row = r;
     }
     if (!two_phase) {
         const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;
