@@ -223,9 +223,6 @@ int plan_build(fcwt_plan* P) {
         d.out_off = (long long)r * sp.n;
         d.out_scale = out_scale;
         d.out_row = r;
-        if (N >= kP2 && rp.K > kMaxK)
-            return fail(FCWT_ERR_UNSUPPORTED,
-                        "row support wider than 32768 bins at N > 16384 is not implemented in this build");
     }
     P->two_phase = N > kMaxFusedN;
     if (!P->two_phase) {
@@ -240,17 +237,19 @@ int plan_build(fcwt_plan* P) {
         S = std::min(S, std::max(1, P->n_rows));
         int D = std::max(1, std::min(tc.lag, S / 2));
         if (S == 1) D = 1;
-        const int n_a = kP2 / kChunk;
         const int n_b = M / kGroupCols;
         for (int r = 0; r < P->n_rows; r++) {
+            const bool wide = rows[(size_t)r].K > kMaxK;
             rows[(size_t)r].slot = r % S;
             rows[(size_t)r].wait_row = r >= S ? r - S : -1;
-            rows[(size_t)r].n_a = n_a;
+            rows[(size_t)r].n_a = wide ? kP2 / kWideChunk : kP2 / kChunk;
             rows[(size_t)r].n_b = n_b;
         }
         for (int step = 0; step < P->n_rows + D; step++) {
-            if (step < P->n_rows)
-                for (int a = 0; a < n_a; a++) items.push_back({ITEM_PHASE1, step, a, 0});
+            if (step < P->n_rows) {
+                const int type = rows[(size_t)step].K > kMaxK ? ITEM_PHASE1W : ITEM_PHASE1;
+                for (int a = 0; a < rows[(size_t)step].n_a; a++) items.push_back({type, step, a, 0});
+            }
             const int rb = step - D;
             if (rb >= 0 && rb < P->n_rows)
                 for (int b = 0; b < n_b; b++) items.push_back({ITEM_PHASE2, rb, b, 0});

@@ -63,7 +63,11 @@ struct RowDesc {
     int out_row;      // row index inside that buffer (for tensor-map stores)
 };
 
-enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3 };
+enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3, ITEM_PHASE1W = 4 };
+
+// Rows whose window needs K > kMaxK use warp-cooperative phase-1 items: each
+// covers kWideChunk consecutive k2 (one per warp) for all v.
+constexpr int kWideChunk = kThreads / 32;
 
 struct Item {
     int type;

@@ -297,6 +297,76 @@ __device__ void phase1_chunk_dispatch(int K, const SigDesc& S, const RowDesc& R,
     }
 }
 
+// Phase 1 of a wide row (K = 32*K2 > 32): warp w handles k2 = k2_0 + w; for
+// every v the warp runs the K-point DFT cooperatively (in-lane K2-point DFT
+// over j, twiddle w_K^{l p}, SMEM transpose, FFT32 over l on lanes p < K2,
+// output u = p + K2 q), the CTA stages the 8 k2 columns of outputs and writes
+// G[v + R u][k2_0 .. k2_0+7] in 64-byte runs with the w_N^{(k2+L) c} twiddle.
+template <int K2>
+__device__ void phase1_wide(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
+                            const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                            float2* __restrict__ region0, float2* __restrict__ G) {
+    constexpr int K = 32 * K2;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int log2N = S.log2N;
+    const int N = 1 << log2N;
+    const unsigned Nm = (unsigned)N - 1u;
+    const int M = N >> kLog2P2;
+    const int Rr = M / K;
+    const float nm1 = (float)N - 1.0f;
+    const int k2 = k2_0 + warp;
+    float2* tb = region0 + warp * (32 * 33);
+    for (int v = 0; v < Rr; v++) {
+        float2 z[K2];
+#pragma unroll
+        for (int j = 0; j < K2; j++) {
+            const int k1 = lane + 32 * j;
+            float2 a = bin_value(R, S, pool, nm1, R.L + k2 + kP2 * k1);
+            if (v != 0) a = cmul(a, twhi[v * k1]);
+            z[j] = a;
+        }
+        fft_reg<K2, +1>(z);
+#pragma unroll
+        for (int p = 1; p < K2; p++) z[p] = cmul(z[p], twhi[(lane * p * Rr) & (M - 1)]);
+#pragma unroll
+        for (int p = 0; p < K2; p++) tb[p * 33 + lane] = z[p];
+        __syncwarp();
+        float2 y[32];
+        if (lane < K2) {
+#pragma unroll
+            for (int l = 0; l < 32; l++) y[l] = tb[lane * 33 + l];
+            fft_reg<32, +1>(y);
+        }
+        __syncthreads();  // all transposes done before staging overwrites region0
+        if (lane < K2) {
+#pragma unroll
+            for (int q = 0; q < 32; q++) region0[(lane + K2 * q) * kWideChunk + warp] = y[q];
+        }
+        __syncthreads();
+        for (int idx = tid; idx < K * kWideChunk; idx += kThreads) {
+            const int u = idx / kWideChunk;
+            const int w = idx - u * kWideChunk;
+            const int c = v + Rr * u;
+            const unsigned e = ((unsigned)(k2_0 + w + R.L) * (unsigned)c) & Nm;
+            __stcg(G + (size_t)c * kP2 + k2_0 + w, cmul(region0[idx], tw_n(twlo, twhi, e)));
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void phase1_wide_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool, int k2_0,
+                                     const float2* twlo, const float2* twhi, float2* region0, float2* G) {
+    switch (K) {
+        case 64: phase1_wide<2>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 128: phase1_wide<4>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 256: phase1_wide<8>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 512: phase1_wide<16>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        default: phase1_wide<32>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+    }
+}
+
 // Warp-level 1024-point DFT (sign +): on entry lane l holds x[m] = G[l + 32 m];
 // on exit lane l holds x[h] = Y[l + 32 h]. tbuf: 32*33 float2 of this warp.
 __device__ __forceinline__ void dft1024_warp(float2 (&x)[32], int lane, float2* __restrict__ tbuf,
@@ -428,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const float2* twhi = (Mcols <= kTwhiSmem) ? twhi_s : S.tw + kP2;
 
         // region0 may still be read by the bulk stores of the previous phase-2 item
-        if (P.tma_store && (item.type == ITEM_PHASE2 || item.type == ITEM_FUSED)) {
+        if (P.tma_store && (item.type == ITEM_PHASE2 || item.type == ITEM_FUSED || item.type == ITEM_PHASE1W)) {
             if (tid == 0) bulk_wait_read_all();
             __syncthreads();
         }
@@ -491,6 +561,21 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (s_ok) {
                 float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
                 phase1_chunk_dispatch<true>(R.K, S, R, P.stale_pool, item.part * kChunk, zs, twlo, twhi, G);
+                if (tid == 0) {
+                    __threadfence();
+                    red_release_add(a_done + item.row, 1u);
+                }
+            }
+        } else if (item.type == ITEM_PHASE1W) {
+            if (tid == 0) {
+                s_ok = 1;
+                if (R.wait_row >= 0)
+                    s_ok = wait_counter(b_done + R.wait_row, (unsigned)P.rows[R.wait_row].n_b, P.err) ? 1 : 0;
+            }
+            __syncthreads();
+            if (s_ok) {
+                float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
+                phase1_wide_dispatch(R.K, S, R, P.stale_pool, item.part * kWideChunk, twlo, twhi, region0, G);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(a_done + item.row, 1u);
