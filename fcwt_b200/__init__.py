@@ -7,8 +7,8 @@ boilerplate). The transform runs in hand-written CUDA kernels behind the C ABI
 of lib/libfcwt_b200.so; there is no CPU fallback.
 """
 from ._lib import FcwtError, FCWT_OUT_BF16, FCWT_OUT_C64, FCWT_OUT_F16, LIB_PATH  # noqa: F401
-from .api import (FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, Morlet, Plan, Scales,  # noqa: F401
-                  Wavelet, cwt, cwt_device, mother_host, row_truncation, synchronize)
+from .api import (FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, BatchPlan, Morlet, Plan,  # noqa: F401
+                  Scales, Wavelet, cwt, cwt_device, mother_host, row_truncation, synchronize)
 
 __all__ = ["Morlet", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
-           "cwt_device", "Plan", "synchronize", "row_truncation", "mother_host", "FcwtError"]
+           "cwt_device", "Plan", "BatchPlan", "synchronize", "row_truncation", "mother_host", "FcwtError"]

@@ -56,6 +56,9 @@ SIGNATURES = {
     "fcwt_plan_create": (_i, [_vp, _i, _i, _f, _vp, _i, _i, _u, _i, _i, ctypes.POINTER(_vp)]),
     "fcwt_plan_execute": (_i, [_vp, _vp, _vp, _i]),
     "fcwt_plan_destroy": (_i, [_vp]),
+    "fcwt_plan_create_batched": (_i, [_vp, _i, _vp, _i, _f, _vp, _vp, _i, _u, ctypes.POINTER(_vp)]),
+    "fcwt_plan_execute_batched": (_i, [_vp, _vp, _vp, _i]),
+    "fcwt_plan_execute_graph": (_i, [_vp, _vp, _vp, _i]),
     "fcwt_create_optimization_plan": (_i, [_vp, _i, _i, _i, ctypes.c_char_p]),
     "fcwt_load_optimization_plan": (_i, [_vp, _i, _i, ctypes.c_char_p]),
     "fcwt_cwt_noalloc": (_i, [_vp, _i, _f, _vp, _i, _i, _u, _vp, _vp, ctypes.POINTER(_i)]),

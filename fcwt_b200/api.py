@@ -356,6 +356,83 @@ class Plan:
             pass
 
 
+class BatchPlan:
+    """Many signals (different lengths and scale grids, one Morlet(fb)) in one
+    plan: one forward-FFT launch sequence per padded length and a single
+    persistent row-engine launch for all rows of all signals
+    (fcwt_plan_create_batched). ``execute(..., graph=True)`` replays the whole
+    sequence from a CUDA graph (device tensors only)."""
+
+    def __init__(self, ns, scales_list, fb: float = 2.0, threads: int = 1, norm: bool = True,
+                 complex_input: bool = False, device: int = 0, exact_support: bool = False):
+        self.ctx = _lib.context(device)
+        self.device = device
+        self.ns = [int(v) for v in ns]
+        self.scales = [_scales_array(sc).copy() for sc in scales_list]
+        if len(self.ns) != len(self.scales):
+            raise ValueError("one scale grid per signal")
+        self.fns = [sc.size for sc in self.scales]
+        self.complex_input = complex_input
+        nsig = len(self.ns)
+        flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0)
+        ns_arr = (ctypes.c_int * nsig)(*self.ns)
+        fns_arr = (ctypes.c_int * nsig)(*self.fns)
+        sc_arr = (ctypes.c_void_p * nsig)(*[sc.ctypes.data for sc in self.scales])
+        h = ctypes.c_void_p()
+        _lib.call("fcwt_plan_create_batched", self.ctx.handle, nsig, ns_arr, 1 if complex_input else 0,
+                  ctypes.c_float(fb), sc_arr, fns_arr, int(threads), flags, ctypes.byref(h))
+        self.handle = h
+
+    def outputs_like(self, device=None, out_dtype=None):
+        """Allocate torch outputs [fn_s, n_s] (complex64) for every signal."""
+        import torch
+
+        dev = device if device is not None else f"cuda:{self.device}"
+        return [torch.empty((fn, n), dtype=torch.complex64, device=dev) for fn, n in zip(self.fns, self.ns)]
+
+    def execute(self, inputs, outputs, out_type: int = FCWT_OUT_C64, graph: bool = False, stream=None) -> None:
+        nsig = len(self.ns)
+        if len(inputs) != nsig or len(outputs) != nsig:
+            raise ValueError("one input and one output per signal")
+        torch_mode = any(_is_torch(v) for v in list(inputs) + list(outputs))
+        keep = []
+        ins, outs = [], []
+        for s in range(nsig):
+            x, o = inputs[s], outputs[s]
+            if _is_torch(x):
+                ins.append(x.data_ptr())
+            else:
+                xx = _host_input(x, self.complex_input)
+                keep.append(xx)
+                ins.append(xx.ctypes.data)
+            outs.append(o.data_ptr() if _is_torch(o) else o.ctypes.data)
+        in_arr = (ctypes.c_void_p * nsig)(*ins)
+        out_arr = (ctypes.c_void_p * nsig)(*outs)
+        fname = "fcwt_plan_execute_graph" if graph else "fcwt_plan_execute_batched"
+        if torch_mode:
+            import torch
+
+            st = stream if stream is not None else torch.cuda.current_stream(self.device)
+            self.ctx.set_stream(st.cuda_stream)
+            try:
+                _lib.call(fname, self.handle, in_arr, out_arr, out_type)
+            finally:
+                self.ctx.set_stream(None)
+        else:
+            _lib.call(fname, self.handle, in_arr, out_arr, out_type)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) and self.handle.value:
+            _lib.load().fcwt_plan_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def synchronize(device: int = 0) -> None:
     """Wait for the device work of this process's context and raise on device errors."""
     _lib.context(device).synchronize()

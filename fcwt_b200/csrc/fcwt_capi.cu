@@ -24,6 +24,8 @@ cudaError_t launch_mother(float fb, int N, float norm, float* out, cudaStream_t 
 cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st);
 cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
                            float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
+cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                                   int* n_kernels);
 cudaError_t engine_configure();
 cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
@@ -155,16 +157,38 @@ struct fcwt_context {
     long long kernel_launches = 0;
 };
 
+// One signal of a plan.
+struct PlanSignal {
+    fcwt::SignalPlan sp;
+    int rb = 0, re = 0;  // rows of this signal produced by the plan
+    int row0 = 0;        // global index of its first produced row
+    int table = 0;       // index into fcwt_plan::tables
+    DevBuf X;            // forward spectrum, N complex
+};
+
+// Tables shared by all signals of one padded length.
+struct PlanTables {
+    int log2N = 0;
+    DevBuf mother, tw;
+};
+
 struct fcwt_plan {
     fcwt_context* ctx = nullptr;
-    fcwt::SignalPlan sp;
-    int rb = 0, re = 0;
-    DevBuf X, mother, tw, pool, sigs, rows, items;
+    float fb = 0;
+    bool is_complex = false;
+    std::vector<PlanSignal> sig;
+    std::vector<PlanTables> tables;
+    DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs;
+    fcwt::FwdJob* jobs_host = nullptr;  // pinned staging of the batched forward jobs
     int n_items = 0;
     int n_rows = 0;
     int slots = 0;
     long long slot_elems = 0;
     bool two_phase = false;
+    // CUDA graph of the last device-resident batched execution
+    cudaGraphExec_t graph = nullptr;
+    std::vector<const void*> graph_key;
+    int graph_out_type = -1;
 };
 
 namespace {
@@ -177,154 +201,241 @@ int ctx_prepare(fcwt_context* ctx) {
 
 void plan_free(fcwt_plan* p) {
     if (!p) return;
-    p->X.release();
-    p->mother.release();
-    p->tw.release();
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    for (auto& s : p->sig) s.X.release();
+    for (auto& t : p->tables) {
+        t.mother.release();
+        t.tw.release();
+    }
     p->pool.release();
     p->sigs.release();
     p->rows.release();
     p->items.release();
+    p->fwd_jobs.release();
+    p->fwd_tmp.release();
+    p->graph_jobs.release();
+    if (p->jobs_host) cudaFreeHost(p->jobs_host);
     delete p;
 }
 
-// Builds the work list: small / fused rows get one item each; two-phase rows
-// get n_a phase-1 items and n_b phase-2 items, phase 2 of row r issued after
-// phase 1 of row r + lag, scratch slots reused round-robin.
+// Builds descriptors and the work list of all signals. Rows of N < 1024 get a
+// direct-DFT item, rows of N <= 8192 one fused item; two-phase rows (all
+// signals, in order) get phase-1 items and phase-2 items, phase 2 of row r
+// issued after phase 1 of row r + lag, scratch slots reused round-robin.
 int plan_build(fcwt_plan* P) {
     using namespace fcwt;
     fcwt_context* ctx = P->ctx;
-    const SignalPlan& sp = P->sp;
-    const int N = sp.N;
-    const int M = sp.M;
-    P->n_rows = P->re - P->rb;
-    std::vector<RowDesc> rows((size_t)P->n_rows);
-    std::vector<Item> items;
-    // stale pool: concatenated tables
-    std::vector<float> pool;
-    pool.reserve(sp.tables.size() * (size_t)sp.half);
-    for (const auto& T : sp.tables) pool.insert(pool.end(), T.begin(), T.end());
-    const float out_scale = (sp.flags & kFlagNorm) ? 1.0f / (float)N : 1.0f;
-    for (int r = 0; r < P->n_rows; r++) {
-        const RowPlan& rp = sp.rows[(size_t)(P->rb + r)];
-        RowDesc& d = rows[(size_t)r];
-        d.sig = 0;
-        d.proc = rp.proc;
-        d.step = rp.step;
-        d.K = rp.K;
-        d.L = rp.L;
-        d.lo = rp.lo;
-        d.hi = rp.hi;
-        d.stale = rp.table >= 0 ? rp.table * sp.half : -1;
-        d.slot = -1;
-        d.wait_row = -1;
-        d.n_a = 0;
-        d.n_b = 0;
-        d.out_buf = 0;
-        d.out_off = (long long)r * sp.n;
-        d.out_scale = out_scale;
-        d.out_row = r;
+    cudaStream_t st = ctx->stream;
+    const int nsig = (int)P->sig.size();
+    if (nsig > kMaxOuts) return fail(FCWT_ERR_INVALID, "at most 1024 signals per plan");
+    // tables per padded length
+    for (auto& S : P->sig) {
+        int t = -1;
+        for (size_t i = 0; i < P->tables.size(); i++)
+            if (P->tables[i].log2N == S.sp.log2N) t = (int)i;
+        if (t < 0) {
+            P->tables.emplace_back();
+            P->tables.back().log2N = S.sp.log2N;
+            t = (int)P->tables.size() - 1;
+        }
+        S.table = t;
     }
-    P->two_phase = N > kMaxFusedN;
-    if (!P->two_phase) {
-        const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;
-        for (int r = 0; r < P->n_rows; r++) items.push_back({type, r, 0, 0});
-        P->slots = 0;
-        P->slot_elems = 0;
-    } else {
-        const TuneChoice& tc = ctx->tune[sp.log2N];
-        const long long slot_bytes = (long long)N * 8;
-        int S = (int)std::max(4LL, std::min(40LL, ((long long)tc.scratch_mb << 20) / slot_bytes));
-        S = std::min(S, std::max(1, P->n_rows));
+    std::vector<float> pool;
+    std::vector<RowDesc> rows;
+    std::vector<int> two_phase_rows;  // global indices, in order
+    std::vector<Item> items;
+    int max_two_phase_log2N = 0;
+    for (int s = 0; s < nsig; s++) {
+        PlanSignal& S = P->sig[(size_t)s];
+        const SignalPlan& sp = S.sp;
+        const long long pool_off = (long long)pool.size();
+        for (const auto& T : sp.tables) pool.insert(pool.end(), T.begin(), T.end());
+        if ((long long)pool.size() > (1ll << 30)) return fail(FCWT_ERR_INVALID, "stale-bin tables too large");
+        const float out_scale = (sp.flags & kFlagNorm) ? 1.0f / (float)sp.N : 1.0f;
+        S.row0 = (int)rows.size();
+        for (int r = S.rb; r < S.re; r++) {
+            const RowPlan& rp = sp.rows[(size_t)r];
+            RowDesc d;
+            std::memset(&d, 0, sizeof(d));
+            d.sig = s;
+            d.proc = rp.proc;
+            d.step = rp.step;
+            d.K = rp.K;
+            d.L = rp.L;
+            d.lo = rp.lo;
+            d.hi = rp.hi;
+            d.stale = rp.table >= 0 ? (int)(pool_off + (long long)rp.table * sp.half) : -1;
+            d.slot = -1;
+            d.wait_row = -1;
+            d.out_buf = s;
+            d.out_off = (long long)(r - S.rb) * sp.n;
+            d.out_scale = out_scale;
+            d.out_row = r - S.rb;
+            const int g = (int)rows.size();
+            rows.push_back(d);
+            if (sp.N > kMaxFusedN) {
+                two_phase_rows.push_back(g);
+                max_two_phase_log2N = std::max(max_two_phase_log2N, sp.log2N);
+            } else {
+                items.push_back({sp.N < kP2 ? ITEM_SMALL : ITEM_FUSED, g, 0, 0});
+            }
+        }
+    }
+    P->n_rows = (int)rows.size();
+    P->two_phase = !two_phase_rows.empty();
+    P->slots = 0;
+    P->slot_elems = 0;
+    if (P->two_phase) {
+        const TuneChoice& tc = ctx->tune[max_two_phase_log2N];
+        const long long slot_elems = 1ll << max_two_phase_log2N;
+        const int nt = (int)two_phase_rows.size();
+        int S = (int)std::max(4LL, std::min(40LL, ((long long)tc.scratch_mb << 20) / (slot_elems * 8)));
+        S = std::min(S, std::max(1, nt));
         int D = std::max(1, std::min(tc.lag, S / 2));
         if (S == 1) D = 1;
-        const int n_b = M / kGroupCols;
-        for (int r = 0; r < P->n_rows; r++) {
-            const bool wide = rows[(size_t)r].K > kMaxK;
-            rows[(size_t)r].slot = r % S;
-            rows[(size_t)r].wait_row = r >= S ? r - S : -1;
-            rows[(size_t)r].n_a = wide ? kP2 / kWideChunk : kP2 / kChunk;
-            rows[(size_t)r].n_b = n_b;
+        if (D >= S && S > 1) return fail(FCWT_ERR_INVALID, "internal: lag >= slots");
+        for (int i = 0; i < nt; i++) {
+            RowDesc& d = rows[(size_t)two_phase_rows[(size_t)i]];
+            const int M = (int)(1ll << (P->sig[(size_t)d.sig].sp.log2N - kLog2P2));
+            d.slot = i % S;
+            d.wait_row = i >= S ? two_phase_rows[(size_t)(i - S)] : -1;
+            d.n_a = d.K > kMaxK ? kP2 / kWideChunk : kP2 / kChunk;
+            d.n_b = M / kGroupCols;
         }
-        for (int step = 0; step < P->n_rows + D; step++) {
-            if (step < P->n_rows) {
-                const int type = rows[(size_t)step].K > kMaxK ? ITEM_PHASE1W : ITEM_PHASE1;
-                for (int a = 0; a < rows[(size_t)step].n_a; a++) items.push_back({type, step, a, 0});
+        for (int step = 0; step < nt + D; step++) {
+            if (step < nt) {
+                const int g = two_phase_rows[(size_t)step];
+                const int type = rows[(size_t)g].K > kMaxK ? ITEM_PHASE1W : ITEM_PHASE1;
+                for (int a = 0; a < rows[(size_t)g].n_a; a++) items.push_back({type, g, a, 0});
             }
             const int rb = step - D;
-            if (rb >= 0 && rb < P->n_rows)
-                for (int b = 0; b < n_b; b++) items.push_back({ITEM_PHASE2, rb, b, 0});
+            if (rb >= 0 && rb < nt) {
+                const int g = two_phase_rows[(size_t)rb];
+                for (int b = 0; b < rows[(size_t)g].n_b; b++) items.push_back({ITEM_PHASE2, g, b, 0});
+            }
         }
         P->slots = S;
-        P->slot_elems = N;
-        // the lag must not exceed the slot count (phase 1 of row r waits on
-        // phase 2 of row r - S, which must already be issued)
-        if (D >= S && S > 1) return fail(FCWT_ERR_INVALID, "internal: lag >= slots");
+        P->slot_elems = slot_elems;
     }
     P->n_items = (int)items.size();
 
-    cudaStream_t st = ctx->stream;
-    FCWT_CUDA_TRY(P->X.ensure((size_t)N * sizeof(float2)));
-    FCWT_CUDA_TRY(P->mother.ensure((size_t)N * sizeof(float)));
-    const int tw_n = 1024 + std::max(M, 1);
-    FCWT_CUDA_TRY(P->tw.ensure((size_t)tw_n * sizeof(float2)));
+    // device buffers and tables
+    for (auto& T : P->tables) {
+        const int N = 1 << T.log2N;
+        const int M = N >= kP2 ? N / kP2 : 1;
+        FCWT_CUDA_TRY(T.mother.ensure((size_t)N * sizeof(float)));
+        FCWT_CUDA_TRY(T.tw.ensure((size_t)(1024 + M) * sizeof(float2)));
+        FCWT_CUDA_TRY(launch_mother(P->fb, N, host::mother_norm(), T.mother.as<float>(), st));
+        FCWT_CUDA_TRY(launch_twiddle(T.log2N, T.tw.as<float2>(), st));
+    }
+    std::vector<SigDesc> sds((size_t)nsig);
+    size_t tmp_elems = 0;
+    for (int s = 0; s < nsig; s++) {
+        PlanSignal& S = P->sig[(size_t)s];
+        FCWT_CUDA_TRY(S.X.ensure((size_t)S.sp.N * sizeof(float2)));
+        sds[(size_t)s].X = S.X.as<float2>();
+        sds[(size_t)s].mother = P->tables[(size_t)S.table].mother.as<float>();
+        sds[(size_t)s].tw = P->tables[(size_t)S.table].tw.as<float2>();
+        sds[(size_t)s].log2N = S.sp.log2N;
+        sds[(size_t)s].n = S.sp.n;
+        tmp_elems += (size_t)S.sp.N;
+    }
+    if (nsig > 1) {
+        FCWT_CUDA_TRY(P->fwd_tmp.ensure(tmp_elems * sizeof(float2)));
+        FCWT_CUDA_TRY(P->fwd_jobs.ensure((size_t)nsig * sizeof(FwdJob)));
+        FCWT_CUDA_TRY(cudaMallocHost(&P->jobs_host, (size_t)nsig * sizeof(FwdJob)));
+    }
     FCWT_CUDA_TRY(P->pool.ensure(std::max<size_t>(pool.size(), 1) * sizeof(float)));
-    FCWT_CUDA_TRY(P->sigs.ensure(sizeof(SigDesc)));
+    FCWT_CUDA_TRY(P->sigs.ensure(sds.size() * sizeof(SigDesc)));
     FCWT_CUDA_TRY(P->rows.ensure(std::max<size_t>(rows.size(), 1) * sizeof(RowDesc)));
     FCWT_CUDA_TRY(P->items.ensure(std::max<size_t>(items.size(), 1) * sizeof(Item)));
-    FCWT_CUDA_TRY(launch_mother(sp.fb, N, host::mother_norm(), P->mother.as<float>(), st));
-    FCWT_CUDA_TRY(launch_twiddle(sp.log2N, P->tw.as<float2>(), st));
-    SigDesc sd;
-    sd.X = P->X.as<float2>();
-    sd.mother = P->mother.as<float>();
-    sd.tw = P->tw.as<float2>();
-    sd.log2N = sp.log2N;
-    sd.n = sp.n;
     if (!pool.empty())
-        FCWT_CUDA_TRY(cudaMemcpyAsync(P->pool.p, pool.data(), pool.size() * sizeof(float),
-                                      cudaMemcpyHostToDevice, st));
-    FCWT_CUDA_TRY(cudaMemcpyAsync(P->sigs.p, &sd, sizeof(sd), cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->pool.p, pool.data(), pool.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(cudaMemcpyAsync(P->sigs.p, sds.data(), sds.size() * sizeof(SigDesc), cudaMemcpyHostToDevice, st));
     if (!rows.empty())
-        FCWT_CUDA_TRY(cudaMemcpyAsync(P->rows.p, rows.data(), rows.size() * sizeof(RowDesc),
-                                      cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->rows.p, rows.data(), rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
     if (!items.empty())
-        FCWT_CUDA_TRY(cudaMemcpyAsync(P->items.p, items.data(), items.size() * sizeof(Item),
-                                      cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->items.p, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice, st));
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;
 }
 
-int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
+// (table, count) groups of the batched forward jobs, in table order.
+void job_groups(const fcwt_plan* P, std::vector<std::pair<int, int>>& groups) {
+    groups.clear();
+    for (size_t t = 0; t < P->tables.size(); t++) {
+        int c = 0;
+        for (const auto& S : P->sig) c += S.table == (int)t;
+        groups.push_back({(int)t, c});
+    }
+}
+
+// Fills P->jobs_host with the forward jobs of all signals ordered by table.
+void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int, int>>& groups) {
+    using namespace fcwt;
+    const int nsig = (int)P->sig.size();
+    std::vector<size_t> tmp_off((size_t)nsig);
+    size_t acc = 0;
+    for (int s = 0; s < nsig; s++) {
+        tmp_off[(size_t)s] = acc;
+        acc += (size_t)P->sig[(size_t)s].sp.N;
+    }
+    int k = 0;
+    for (size_t t = 0; t < P->tables.size(); t++) {
+        for (int s = 0; s < nsig; s++) {
+            PlanSignal& S = P->sig[(size_t)s];
+            if (S.table != (int)t) continue;
+            FwdJob& j = P->jobs_host[k++];
+            j.in_r = S.sp.is_complex ? nullptr : (const float*)din[s];
+            j.in_c = S.sp.is_complex ? (const float2*)din[s] : nullptr;
+            j.n = S.sp.n;
+            j.pad = 0;
+            j.X = S.X.as<float2>();
+            j.tmp = P->fwd_tmp.as<float2>() + tmp_off[(size_t)s];
+        }
+    }
+    job_groups(P, groups);
+}
+
+// Enqueues the forward FFTs and the row engine for device-resident inputs and
+// outputs (no host synchronisation, so it can be captured into a graph).
+// graph_jobs: device copy of the forward jobs prepared before a capture.
+int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int out_type, bool allow_profiling,
+                 const fcwt::FwdJob* graph_jobs = nullptr) {
     using namespace fcwt;
     fcwt_context* ctx = P->ctx;
-    int rc = ctx_prepare(ctx);
-    if (rc) return rc;
-    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
-        return fail(FCWT_ERR_INVALID, "unknown output type");
-    const SignalPlan& sp = P->sp;
-    const int n = sp.n;
-    if (n == 0 || P->n_rows == 0) return FCWT_OK;
-    if (!input || !output) return fail(FCWT_ERR_INVALID, "null input or output pointer");
     cudaStream_t st = ctx->stream;
-    const size_t in_bytes = (size_t)n * (sp.is_complex ? 8 : 4);
-    const size_t out_bytes = (size_t)P->n_rows * (size_t)n * out_elem_bytes(out_type);
-    const void* din = input;
-    if (!is_device_pointer(input)) {
-        FCWT_CUDA_TRY(ctx->in_stage.ensure(in_bytes));
-        FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->in_stage.p, input, in_bytes, cudaMemcpyHostToDevice, st));
-        din = ctx->in_stage.p;
+    const int nsig = (int)P->sig.size();
+    if (nsig == 1) {
+        PlanSignal& S = P->sig[0];
+        FCWT_CUDA_TRY(ctx->tmp.ensure((size_t)S.sp.N * sizeof(float2)));
+        int n_fwd = 0;
+        FCWT_CUDA_TRY(launch_forward(S.sp.is_complex ? nullptr : (const float*)din[0],
+                                     S.sp.is_complex ? (const float2*)din[0] : nullptr, S.sp.n, S.sp.log2N,
+                                     P->tables[(size_t)S.table].tw.as<float2>(), S.X.as<float2>(),
+                                     ctx->tmp.as<float2>(), st, &n_fwd));
+        ctx->kernel_launches += n_fwd;
+    } else {
+        // batched forward FFTs, one launch sequence per padded length
+        std::vector<std::pair<int, int>> groups;
+        const FwdJob* djobs = graph_jobs;
+        if (!djobs) {
+            build_jobs(P, din, groups);
+            FCWT_CUDA_TRY(cudaMemcpyAsync(P->fwd_jobs.p, P->jobs_host, (size_t)nsig * sizeof(FwdJob),
+                                          cudaMemcpyHostToDevice, st));
+            djobs = P->fwd_jobs.as<FwdJob>();
+        } else {
+            job_groups(P, groups);
+        }
+        int off = 0;
+        for (auto& g : groups) {
+            int n_fwd = 0;
+            FCWT_CUDA_TRY(launch_forward_batched(djobs + off, g.second, P->tables[(size_t)g.first].log2N,
+                                                 P->tables[(size_t)g.first].tw.as<float2>(), st, &n_fwd));
+            ctx->kernel_launches += n_fwd;
+            off += g.second;
+        }
     }
-    const bool host_out = !is_device_pointer(output);
-    void* dout = output;
-    if (host_out) {
-        FCWT_CUDA_TRY(ctx->out_stage.ensure(out_bytes));
-        dout = ctx->out_stage.p;
-    }
-    FCWT_CUDA_TRY(ctx->tmp.ensure((size_t)sp.N * sizeof(float2)));
-    int n_fwd = 0;
-    FCWT_CUDA_TRY(launch_forward(sp.is_complex ? nullptr : (const float*)din,
-                                 sp.is_complex ? (const float2*)din : nullptr, n, sp.log2N,
-                                 P->tw.as<float2>(), P->X.as<float2>(), ctx->tmp.as<float2>(), st, &n_fwd));
-    ctx->kernel_launches += n_fwd;
     const size_t n_counters = 1 + 2 * (size_t)P->n_rows;
     FCWT_CUDA_TRY(ctx->counters.ensure(n_counters * sizeof(unsigned)));
     FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, n_counters * sizeof(unsigned), st));
@@ -343,16 +454,20 @@ int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
     ep.slot_elems = P->slot_elems;
     ep.counters = ctx->counters.as<unsigned>();
     ep.n_rows = P->n_rows;
-    ep.outs[0] = dout;
+    for (int s = 0; s < nsig; s++) ep.outs[s] = dout[s];
     ep.out_type = out_type;
     ep.err = ctx->err.as<int>();
     CUtensorMap omap;
     std::memset(&omap, 0, sizeof(omap));
-    ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64 &&
-                    encode_output_map(dout, n, sp.M, P->n_rows, &omap)) ? 1 : 0;
+    if (nsig == 1) {
+        const PlanSignal& S = P->sig[0];
+        ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64 &&
+                        encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap)) ? 1 : 0;
+    }
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
-    if (ctx->profiling) {
+    const bool prof = ctx->profiling && allow_profiling;
+    if (prof) {
         if (!ctx->ev_free.empty()) {
             ev = ctx->ev_free.back();
             ctx->ev_free.pop_back();
@@ -364,18 +479,76 @@ int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
     }
     FCWT_CUDA_TRY(launch_engine(ep, omap, grid, st));
     ctx->kernel_launches += 1;
-    if (ctx->profiling) {
+    if (prof) {
         FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
         ctx->ev_used.push_back(ev);
     }
     FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (host_out) {
-        FCWT_CUDA_TRY(cudaMemcpyAsync(output, dout, out_bytes, cudaMemcpyDeviceToHost, st));
+    return FCWT_OK;
+}
+
+// Runs a plan on host or device buffers: host inputs are staged in, host
+// outputs are copied back (and the call waits for them).
+int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs, int out_type) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
+        return fail(FCWT_ERR_INVALID, "unknown output type");
+    if (P->n_rows == 0) return FCWT_OK;
+    const int nsig = (int)P->sig.size();
+    if (!inputs || !outputs) return fail(FCWT_ERR_INVALID, "null input or output array");
+    cudaStream_t st = ctx->stream;
+    std::vector<const void*> din((size_t)nsig);
+    std::vector<void*> dout((size_t)nsig);
+    std::vector<size_t> out_bytes((size_t)nsig), out_off((size_t)nsig);
+    size_t in_total = 0, out_total = 0;
+    std::vector<size_t> in_off((size_t)nsig);
+    for (int s = 0; s < nsig; s++) {
+        const PlanSignal& S = P->sig[(size_t)s];
+        if (S.re == S.rb || S.sp.n == 0) continue;
+        if (!inputs[s] || !outputs[s]) return fail(FCWT_ERR_INVALID, "null input or output pointer");
+        in_off[(size_t)s] = in_total;
+        if (!is_device_pointer(inputs[s])) in_total += ((size_t)S.sp.n * (S.sp.is_complex ? 8 : 4) + 255) & ~(size_t)255;
+        out_off[(size_t)s] = out_total;
+        out_bytes[(size_t)s] = (size_t)(S.re - S.rb) * (size_t)S.sp.n * out_elem_bytes(out_type);
+        if (!is_device_pointer(outputs[s])) out_total += (out_bytes[(size_t)s] + 255) & ~(size_t)255;
+    }
+    if (in_total) FCWT_CUDA_TRY(ctx->in_stage.ensure(in_total));
+    if (out_total) FCWT_CUDA_TRY(ctx->out_stage.ensure(out_total));
+    bool any_host_out = false;
+    for (int s = 0; s < nsig; s++) {
+        const PlanSignal& S = P->sig[(size_t)s];
+        din[(size_t)s] = inputs[s];
+        dout[(size_t)s] = outputs[s];
+        if (S.re == S.rb || S.sp.n == 0) continue;
+        if (!is_device_pointer(inputs[s])) {
+            void* d = (char*)ctx->in_stage.p + in_off[(size_t)s];
+            FCWT_CUDA_TRY(cudaMemcpyAsync(d, inputs[s], (size_t)S.sp.n * (S.sp.is_complex ? 8 : 4),
+                                          cudaMemcpyHostToDevice, st));
+            din[(size_t)s] = d;
+        }
+        if (!is_device_pointer(outputs[s])) {
+            dout[(size_t)s] = (char*)ctx->out_stage.p + out_off[(size_t)s];
+            any_host_out = true;
+        }
+    }
+    rc = plan_enqueue(P, din.data(), dout.data(), out_type, true);
+    if (rc) return rc;
+    if (any_host_out) {
+        for (int s = 0; s < nsig; s++)
+            if (dout[(size_t)s] != outputs[s] && out_bytes[(size_t)s])
+                FCWT_CUDA_TRY(cudaMemcpyAsync(outputs[s], dout[(size_t)s], out_bytes[(size_t)s], cudaMemcpyDeviceToHost, st));
         FCWT_CUDA_TRY(cudaStreamSynchronize(st));
         if (*ctx->err_host != 0)
             return fail(FCWT_ERR_DEVICE, "row engine reported error bits " + std::to_string(*ctx->err_host));
     }
     return FCWT_OK;
+}
+
+int plan_run(fcwt_plan* P, const void* input, void* output, int out_type) {
+    return plan_run_multi(P, &input, &output, out_type);
 }
 
 bool key_match(const fcwt_context::CacheEntry& e, int n, int cplx, float fb, const float* scales, int fn,
@@ -637,10 +810,13 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
         return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
     fcwt_plan* P = new fcwt_plan();
     P->ctx = ctx;
-    P->rb = row_begin;
-    P->re = row_end;
+    P->fb = fb;
+    P->is_complex = is_complex != 0;
+    P->sig.resize(1);
+    P->sig[0].rb = row_begin;
+    P->sig[0].re = row_end;
     std::string err;
-    if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sp, err)) {
+    if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sig[0].sp, err)) {
         delete P;
         return fail(FCWT_ERR_INVALID, err);
     }
@@ -655,9 +831,126 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
     return FCWT_OK;
 }
 
+int fcwt_plan_create_batched(fcwt_context* ctx, int nsig, const int* ns, int is_complex, float fb,
+                             const float* const* scales, const int* fns, int threads, unsigned flags,
+                             fcwt_plan** out) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (!out) return fail(FCWT_ERR_INVALID, "null plan output");
+    *out = nullptr;
+    if (nsig < 1 || nsig > fcwt::kMaxOuts) return fail(FCWT_ERR_INVALID, "nsig must be in [1, 1024]");
+    if (!ns || !scales || !fns) return fail(FCWT_ERR_INVALID, "null array argument");
+    fcwt_plan* P = new fcwt_plan();
+    P->ctx = ctx;
+    P->fb = fb;
+    P->is_complex = is_complex != 0;
+    P->sig.resize((size_t)nsig);
+    for (int s = 0; s < nsig; s++) {
+        if (ns[s] < 0 || fns[s] < 0 || (fns[s] > 0 && !scales[s])) {
+            delete P;
+            return fail(FCWT_ERR_INVALID, "bad size or scales of signal " + std::to_string(s));
+        }
+        std::string err;
+        if (fcwt::plan_signal(ns[s], is_complex != 0, fb, scales[s], fns[s], threads, flags, P->sig[(size_t)s].sp,
+                              err)) {
+            delete P;
+            return fail(FCWT_ERR_INVALID, "signal " + std::to_string(s) + ": " + err);
+        }
+        P->sig[(size_t)s].rb = 0;
+        P->sig[(size_t)s].re = fns[s];
+    }
+    rc = plan_build(P);
+    if (rc) {
+        std::string keep = g_err;
+        plan_free(P);
+        g_err = keep;
+        return rc;
+    }
+    *out = P;
+    return FCWT_OK;
+}
+
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type) {
     if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (plan->sig.size() != 1) return fail(FCWT_ERR_INVALID, "batched plan: use fcwt_plan_execute_batched");
     return plan_run(plan, input, output, out_type);
+}
+
+int fcwt_plan_execute_batched(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type) {
+    if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    return plan_run_multi(plan, inputs, outputs, out_type);
+}
+
+int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type) {
+    if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    fcwt_context* ctx = plan->ctx;
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
+        return fail(FCWT_ERR_INVALID, "unknown output type");
+    if (!inputs || !outputs) return fail(FCWT_ERR_INVALID, "null input or output array");
+    const int nsig = (int)plan->sig.size();
+    std::vector<const void*> key;
+    for (int s = 0; s < nsig; s++) {
+        if (!is_device_pointer(inputs[s]) || !is_device_pointer(outputs[s]))
+            return fail(FCWT_ERR_INVALID, "graph execution needs device inputs and outputs");
+        key.push_back(inputs[s]);
+        key.push_back(outputs[s]);
+    }
+    cudaStream_t st = ctx->stream;
+    if (!plan->graph || key != plan->graph_key || out_type != plan->graph_out_type) {
+        if (plan->graph) {
+            cudaGraphExecDestroy(plan->graph);
+            plan->graph = nullptr;
+        }
+        // make sure every buffer the enqueue touches exists before capturing
+        size_t maxN = 1;
+        for (auto& S : plan->sig) maxN = std::max(maxN, (size_t)S.sp.N);
+        FCWT_CUDA_TRY(ctx->tmp.ensure(maxN * sizeof(float2)));
+        FCWT_CUDA_TRY(ctx->counters.ensure((1 + 2 * (size_t)plan->n_rows) * sizeof(unsigned)));
+        FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
+        if (plan->two_phase)
+            FCWT_CUDA_TRY(ctx->scratch.ensure((size_t)plan->slots * (size_t)plan->slot_elems * sizeof(float2)));
+        const fcwt::FwdJob* gj = nullptr;
+        if (nsig > 1) {
+            std::vector<std::pair<int, int>> groups;
+            build_jobs(plan, inputs, groups);
+            FCWT_CUDA_TRY(plan->graph_jobs.ensure((size_t)nsig * sizeof(fcwt::FwdJob)));
+            FCWT_CUDA_TRY(cudaMemcpyAsync(plan->graph_jobs.p, plan->jobs_host, (size_t)nsig * sizeof(fcwt::FwdJob),
+                                          cudaMemcpyHostToDevice, st));
+            FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+            gj = plan->graph_jobs.as<fcwt::FwdJob>();
+        }
+        // capture on the context's own stream (the legacy default stream
+        // cannot be captured); the graph is then launched on the caller's
+        FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+        cudaGraph_t g = nullptr;
+        cudaStream_t user = ctx->stream;
+        ctx->stream = ctx->own;
+        cudaError_t e = cudaStreamBeginCapture(ctx->own, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            ctx->stream = user;
+            return fail(FCWT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
+        rc = plan_enqueue(plan, inputs, outputs, out_type, false, gj);
+        e = cudaStreamEndCapture(ctx->own, &g);
+        ctx->stream = user;
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(FCWT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&plan->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            plan->graph = nullptr;
+            return fail(FCWT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        plan->graph_key = key;
+        plan->graph_out_type = out_type;
+    }
+    FCWT_CUDA_TRY(cudaGraphLaunch(plan->graph, st));
+    return FCWT_OK;
 }
 
 int fcwt_plan_destroy(fcwt_plan* plan) {
@@ -711,7 +1004,7 @@ int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const cha
     ctx->tune[log2N] = tc;
     // cached plans of that size were built with the old choices
     for (auto it = ctx->cache.begin(); it != ctx->cache.end();) {
-        if (it->plan->sp.log2N == log2N) {
+        if (it->plan->sig[0].sp.log2N == log2N) {
             fcwt_plan_destroy(it->plan);
             it = ctx->cache.erase(it);
         } else {

@@ -78,6 +78,17 @@ struct Item {
 
 enum OutType : int { OUT_C64 = 0, OUT_BF16 = 1, OUT_F16 = 2 };
 
+// One signal of a batched forward FFT: input (real or complex), its length,
+// the spectrum it produces and a ping-pong buffer of N complex values.
+struct FwdJob {
+    const float* in_r;
+    const float2* in_c;
+    int n;
+    int pad;
+    float2* X;
+    float2* tmp;
+};
+
 // Everything the row engine needs for one launch.
 struct EngineParams {
     const SigDesc* sigs;

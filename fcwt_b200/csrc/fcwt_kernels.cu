@@ -97,6 +97,46 @@ __global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restr
 }
 
 
+// Batched Stockham pass: blockIdx.y selects the signal. src/dst: 0 = the
+// signal's input (first pass only), 1 = its spectrum X, 2 = its tmp buffer.
+template <int R>
+__global__ void k_fwd_pass_batched(const FwdJob* __restrict__ jobs, int src_sel, int dst_sel, int log2N, int log2Ns,
+                                   const float2* __restrict__ tw) {
+    const FwdJob J = jobs[blockIdx.y];
+    const int N = 1 << log2N;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N / R) return;
+    const int Ns = 1 << log2Ns;
+    const int k = j & (Ns - 1);
+    const int shift = log2N - log2Ns - ilog2c(R);
+    const float2* src = src_sel == 1 ? J.X : J.tmp;
+    float2* dst = dst_sel == 1 ? J.X : J.tmp;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int idx = j + r * (N / R);
+        float2 a;
+        if (src_sel == 0) {
+            if (idx < J.n)
+                a = J.in_r ? make_float2(__ldg(J.in_r + idx), 0.0f) : __ldg(J.in_c + idx);
+            else
+                a = make_float2(0.0f, 0.0f);
+        } else {
+            a = src[idx];
+        }
+        if (r > 0 && k > 0) {
+            float2 w = tw_lookup(tw, log2N, (unsigned)(r * k) << shift);
+            w.y = -w.y;
+            a = cmul(a, w);
+        }
+        v[r] = a;
+    }
+    fft_reg<R, -1>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; m++) dst[base + m * Ns] = v[m];
+}
+
 // --------------------------------------------------------------- row engine
 
 // Shared-memory layout of the row engine, per CTA (units of float2):
@@ -677,6 +717,45 @@ cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log
         src_r = nullptr;
         log2Ns += dev::ilog2c(R);
         cur ^= 1;
+    }
+    return cudaSuccess;
+}
+
+// Forward FFTs of njobs signals of the same padded length 2^log2N.
+cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                                   int* n_kernels) {
+    *n_kernels = 0;
+    if (njobs <= 0) return cudaSuccess;
+    if (log2N == 0) return cudaErrorInvalidValue;  // N == 1 is handled by the single-signal path
+    const int N = 1 << log2N;
+    int radices[32];
+    int np = 0, rem = log2N;
+    while (rem >= 4) {
+        radices[np++] = 16;
+        rem -= 4;
+    }
+    if (rem == 3) radices[np++] = 8;
+    if (rem == 2) radices[np++] = 4;
+    if (rem == 1) radices[np++] = 2;
+    int log2Ns = 0;
+    int src = 0;
+    for (int p = 0; p < np; p++) {
+        const int R = radices[p];
+        const int dst = ((np - 1 - p) % 2 == 0) ? 1 : 2;  // the last pass lands in X
+        const int threads = N / R;
+        const int tb = threads < 256 ? threads : 256;
+        dim3 grid((threads + tb - 1) / tb, njobs);
+        switch (R) {
+            case 16: dev::k_fwd_pass_batched<16><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            case 8: dev::k_fwd_pass_batched<8><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            case 4: dev::k_fwd_pass_batched<4><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            default: dev::k_fwd_pass_batched<2><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        (*n_kernels)++;
+        src = dst;
+        log2Ns += dev::ilog2c(R);
     }
     return cudaSuccess;
 }

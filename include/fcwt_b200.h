@@ -118,6 +118,22 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type);
 int fcwt_plan_destroy(fcwt_plan* plan);
 
+/* Batched plan: nsig signals (lengths ns[s], scale grids scales[s] of fns[s]
+ * rows, one Morlet(fb)) transformed by one forward-FFT sequence per padded
+ * length and ONE persistent row-engine launch that interleaves the work of
+ * all signals. No reference counterpart (the reference loops FCWT::cwt per
+ * channel); each signal's rows equal FCWT::cwt of that signal. nsig <= 1024. */
+int fcwt_plan_create_batched(fcwt_context* ctx, int nsig, const int* ns, int is_complex, float fb,
+                             const float* const* scales, const int* fns, int threads, unsigned flags,
+                             fcwt_plan** plan);
+/* inputs[s] / outputs[s]: per-signal buffers (host or device; output of
+ * signal s is fns[s] x ns[s] values). */
+int fcwt_plan_execute_batched(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type);
+/* Same, for device buffers only, replayed from a CUDA graph: the first call
+ * (and any call with different pointers or output type) captures the whole
+ * sequence on the context's stream; later calls launch the graph. */
+int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type);
+
 /* ---- tuning files
  * FCWT::create_FFT_optimization_plan(maxsize, flags), src/fcwt/fcwt.cpp:313-374:
  * for N = 2^11 .. 2^ceil(log2 maxsize), times the engine's scheduling
