@@ -11,4 +11,14 @@ from .api import (FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, BatchPlan
                   Scales, Wavelet, cwt, cwt_device, mother_host, row_truncation, synchronize)
 
 __all__ = ["Morlet", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
-           "cwt_device", "Plan", "BatchPlan", "synchronize", "row_truncation", "mother_host", "FcwtError"]
+           "cwt_device", "Plan", "BatchPlan", "synchronize", "row_truncation", "mother_host", "FcwtError",
+           "morlet_cwt", "LearnableMorletCWT"]
+
+
+def __getattr__(name):
+    # the differentiable operator needs torch; import it on first use
+    if name in ("morlet_cwt", "LearnableMorletCWT", "MorletCWTFunction"):
+        from . import autograd
+
+        return getattr(autograd, name)
+    raise AttributeError(name)

@@ -23,6 +23,7 @@ FCWT_ERR_IO = 6
 FCWT_NORM = 1 << 0
 FCWT_SCALAR_TRUNC = 1 << 1
 FCWT_EXACT_SUPPORT = 1 << 2
+FCWT_CONTINUOUS = 1 << 3
 
 FCWT_OUT_C64 = 0
 FCWT_OUT_BF16 = 1
@@ -61,6 +62,8 @@ SIGNATURES = {
     "fcwt_plan_execute_graph": (_i, [_vp, _vp, _vp, _i]),
     "fcwt_create_optimization_plan": (_i, [_vp, _i, _i, _i, ctypes.c_char_p]),
     "fcwt_load_optimization_plan": (_i, [_vp, _i, _i, ctypes.c_char_p]),
+    "fcwt_morlet_cwt_backward": (_i, [_vp, _vp, _i, _i, _f, _vp, _i, _f, _u, _vp, _vp,
+                                      ctypes.POINTER(ctypes.c_double), _vp]),
     "fcwt_cwt_noalloc": (_i, [_vp, _i, _f, _vp, _i, _i, _u, _vp, _vp, ctypes.POINTER(_i)]),
 }
 

@@ -364,7 +364,8 @@ class BatchPlan:
     sequence from a CUDA graph (device tensors only)."""
 
     def __init__(self, ns, scales_list, fb: float = 2.0, threads: int = 1, norm: bool = True,
-                 complex_input: bool = False, device: int = 0, exact_support: bool = False):
+                 complex_input: bool = False, device: int = 0, exact_support: bool = False,
+                 continuous: bool = False):
         self.ctx = _lib.context(device)
         self.device = device
         self.ns = [int(v) for v in ns]
@@ -374,7 +375,8 @@ class BatchPlan:
         self.fns = [sc.size for sc in self.scales]
         self.complex_input = complex_input
         nsig = len(self.ns)
-        flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0)
+        flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0) | \
+            (_lib.FCWT_CONTINUOUS if continuous else 0)
         ns_arr = (ctypes.c_int * nsig)(*self.ns)
         fns_arr = (ctypes.c_int * nsig)(*self.fns)
         sc_arr = (ctypes.c_void_p * nsig)(*[sc.ctypes.data for sc in self.scales])

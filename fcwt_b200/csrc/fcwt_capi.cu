@@ -26,6 +26,14 @@ cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log
                            float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
 cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
                                    int* n_kernels);
+cudaError_t launch_inverse_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                                   int* n_kernels);
+cudaError_t launch_adjoint_accum(const float2* Xs, const float2* Gh, float2* H, const void* rows, int nr, int half,
+                                 long long Nstride, int batch, float cb, float amp, float inv_sigma, double* acc_sigma,
+                                 double* acc_f, cudaStream_t st);
+cudaError_t launch_take_real(const float2* Y, long long Nstride, int n, int batch, float scale, float* gx,
+                             cudaStream_t st);
+int adjoint_rows_per_pass();
 cudaError_t engine_configure();
 cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
@@ -155,6 +163,11 @@ struct fcwt_context {
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;
     long long kernel_launches = 0;
+    // workspace of the differentiable transform's backward
+    DevBuf adj_tw, adj_x, adj_g, adj_tmp, adj_h, adj_jobs, adj_rows, adj_acc;
+    int adj_tw_log2N = -1;
+    void* adj_jobs_host = nullptr;
+    size_t adj_jobs_host_bytes = 0;
 };
 
 // One signal of a plan.
@@ -271,6 +284,10 @@ int plan_build(fcwt_plan* P) {
             d.out_off = (long long)(r - S.rb) * sp.n;
             d.out_scale = out_scale;
             d.out_row = r - S.rb;
+            d.mode = (sp.flags & kFlagContinuous) ? 1 : 0;
+            d.ca = rp.ca;
+            d.cb = rp.cb;
+            d.cnorm = host::mother_norm();
             const int g = (int)rows.size();
             rows.push_back(d);
             if (sp.N > kMaxFusedN) {
@@ -670,6 +687,10 @@ int fcwt_context_destroy(fcwt_context* ctx) {
     ctx->counters.release();
     ctx->err.release();
     if (ctx->err_host) cudaFreeHost(ctx->err_host);
+    for (DevBuf* b : {&ctx->adj_tw, &ctx->adj_x, &ctx->adj_g, &ctx->adj_tmp, &ctx->adj_h, &ctx->adj_jobs,
+                      &ctx->adj_rows, &ctx->adj_acc})
+        b->release();
+    if (ctx->adj_jobs_host) cudaFreeHost(ctx->adj_jobs_host);
     for (auto& ev : ctx->ev_used) {
         cudaEventDestroy(ev.first);
         cudaEventDestroy(ev.second);
@@ -972,6 +993,144 @@ int fcwt_cwt(fcwt_context* ctx, const float* input, int n, float fb, const float
 int fcwt_ccwt(fcwt_context* ctx, const float* input, int n, float fb, const float* scales, int fn,
               int threads, unsigned flags, void* output, int out_type) {
     return transform(ctx, input, n, 1, fb, scales, fn, threads, flags, output, out_type);
+}
+
+int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch, float fb, const float* freqs,
+                             int fn, float fs, unsigned flags, const void* grad_out, float* grad_x, double* grad_fb,
+                             double* grad_freqs) {
+    using namespace fcwt;
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (n < 0 || batch < 0 || fn < 0) return fail(FCWT_ERR_INVALID, "negative size");
+    if (!(fb > 0.0f) || !(fs > 0.0f)) return fail(FCWT_ERR_INVALID, "fb and fs must be positive");
+    if (grad_fb) *grad_fb = 0.0;
+    if (grad_freqs)
+        for (int i = 0; i < fn; i++) grad_freqs[i] = 0.0;
+    if (n == 0 || batch == 0) return FCWT_OK;
+    if (!x || !grad_out || !grad_x || (fn > 0 && !freqs))
+        return fail(FCWT_ERR_INVALID, "null pointer argument");
+    if (!is_device_pointer(x) || !is_device_pointer(grad_out) || !is_device_pointer(grad_x))
+        return fail(FCWT_ERR_INVALID, "x, grad_out and grad_x must be device pointers");
+    const int log2N = host::find2power(n);
+    if (log2N > kMaxLog2N) return fail(FCWT_ERR_INVALID, "signal too long");
+    const int N = 1 << log2N;
+    cudaStream_t st = ctx->stream;
+    const float scale = (flags & FCWT_NORM) ? 1.0f / (float)N : 1.0f;
+    if (N < 2 || fn == 0) {
+        FCWT_CUDA_TRY(cudaMemsetAsync(grad_x, 0, sizeof(float) * (size_t)n * batch, st));
+        return FCWT_OK;
+    }
+    const int half = N / 2;
+    const int RP = adjoint_rows_per_pass();
+    const int nchunks = (fn + RP - 1) / RP;
+    // tables
+    if (ctx->adj_tw_log2N != log2N) {
+        FCWT_CUDA_TRY(ctx->adj_tw.ensure((size_t)(1024 + std::max(N / 1024, 1)) * sizeof(float2)));
+        FCWT_CUDA_TRY(launch_twiddle(log2N, ctx->adj_tw.as<float2>(), st));
+        ctx->adj_tw_log2N = log2N;
+    }
+    const size_t BN = (size_t)batch * N;
+    FCWT_CUDA_TRY(ctx->adj_x.ensure(BN * sizeof(float2)));
+    FCWT_CUDA_TRY(ctx->adj_h.ensure(BN * sizeof(float2)));
+    FCWT_CUDA_TRY(ctx->adj_g.ensure(BN * RP * sizeof(float2)));
+    FCWT_CUDA_TRY(ctx->adj_tmp.ensure(BN * RP * sizeof(float2)));
+    const size_t njobs_total = (size_t)batch * (2 + (size_t)fn);
+    FCWT_CUDA_TRY(ctx->adj_jobs.ensure(njobs_total * sizeof(FwdJob)));
+    if (ctx->adj_jobs_host_bytes < njobs_total * sizeof(FwdJob)) {
+        // the previous backward's uploads must have been consumed before the
+        // pinned staging is replaced
+        FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+        if (ctx->adj_jobs_host) cudaFreeHost(ctx->adj_jobs_host);
+        ctx->adj_jobs_host = nullptr;
+        FCWT_CUDA_TRY(cudaMallocHost(&ctx->adj_jobs_host, njobs_total * sizeof(FwdJob)));
+        ctx->adj_jobs_host_bytes = njobs_total * sizeof(FwdJob);
+    } else {
+        FCWT_CUDA_TRY(cudaStreamSynchronize(st));  // staging reused: earlier uploads must be done
+    }
+    FwdJob* jh = static_cast<FwdJob*>(ctx->adj_jobs_host);
+    FwdJob* jd = ctx->adj_jobs.as<FwdJob>();
+    // per-row constants
+    struct AdjRowH {
+        float ca, dfdq;
+    };
+    std::vector<AdjRowH> rowc((size_t)fn);
+    const double two_pi = 6.283185307179586;
+    for (int i = 0; i < fn; i++) {
+        const double f = freqs[i];
+        if (!(f > 0.0)) return fail(FCWT_ERR_INVALID, "frequencies must be positive");
+        rowc[(size_t)i].ca = (float)(two_pi * fb * (fs / f) / N);
+        rowc[(size_t)i].dfdq = (float)(two_pi * fb / N * fs / (f * f));
+    }
+    FCWT_CUDA_TRY(ctx->adj_rows.ensure(rowc.size() * sizeof(AdjRowH)));
+    FCWT_CUDA_TRY(ctx->adj_acc.ensure((1 + (size_t)fn) * sizeof(double)));
+    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->adj_rows.p, rowc.data(), rowc.size() * sizeof(AdjRowH), cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->adj_acc.p, 0, (1 + (size_t)fn) * sizeof(double), st));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->adj_h.p, 0, BN * sizeof(float2), st));
+    const float2* tw = ctx->adj_tw.as<float2>();
+    int nk = 0;
+    // X_b = FFT(x_b)
+    size_t jo = 0;
+    for (int b = 0; b < batch; b++) {
+        FwdJob& j = jh[jo + b];
+        j.in_r = x + (size_t)b * n;
+        j.in_c = nullptr;
+        j.n = n;
+        j.pad = 0;
+        j.X = ctx->adj_x.as<float2>() + (size_t)b * N;
+        j.tmp = ctx->adj_tmp.as<float2>() + (size_t)b * N;
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(jd + jo, jh + jo, (size_t)batch * sizeof(FwdJob), cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch, log2N, tw, st, &nk));
+    ctx->kernel_launches += nk;
+    jo += batch;
+    // rows in chunks: Ghat = FFT(G), accumulate H and the parameter sums
+    const float2* G = static_cast<const float2*>(grad_out);
+    for (int c = 0; c < nchunks; c++) {
+        const int i0 = c * RP;
+        const int nr = std::min(RP, fn - i0);
+        for (int b = 0; b < batch; b++) {
+            for (int i = 0; i < nr; i++) {
+                FwdJob& j = jh[jo + (size_t)b * nr + i];
+                j.in_r = nullptr;
+                j.in_c = G + ((size_t)b * fn + i0 + i) * n;
+                j.n = n;
+                j.pad = 0;
+                j.X = ctx->adj_g.as<float2>() + ((size_t)b * nr + i) * N;
+                j.tmp = ctx->adj_tmp.as<float2>() + ((size_t)b * nr + i) * N;
+            }
+        }
+        FCWT_CUDA_TRY(cudaMemcpyAsync(jd + jo, jh + jo, (size_t)batch * nr * sizeof(FwdJob), cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch * nr, log2N, tw, st, &nk));
+        ctx->kernel_launches += nk;
+        jo += (size_t)batch * nr;
+        FCWT_CUDA_TRY(launch_adjoint_accum(ctx->adj_x.as<float2>(), ctx->adj_g.as<float2>(), ctx->adj_h.as<float2>(),
+                                           static_cast<const AdjRowH*>(ctx->adj_rows.p) + i0, nr, half, N, batch,
+                                           (float)(two_pi * fb), host::mother_norm(), 1.0f / fb,
+                                           ctx->adj_acc.as<double>(), ctx->adj_acc.as<double>() + 1 + i0, st));
+        ctx->kernel_launches += 1;
+    }
+    // dL/dx = Re(scale * IFFTraw(H))[0:n]
+    for (int b = 0; b < batch; b++) {
+        FwdJob& j = jh[jo + b];
+        j.in_r = nullptr;
+        j.in_c = ctx->adj_h.as<float2>() + (size_t)b * N;
+        j.n = N;
+        j.pad = 0;
+        j.X = ctx->adj_g.as<float2>() + (size_t)b * N;
+        j.tmp = ctx->adj_tmp.as<float2>() + (size_t)b * N;
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(jd + jo, jh + jo, (size_t)batch * sizeof(FwdJob), cudaMemcpyHostToDevice, st));
+    FCWT_CUDA_TRY(launch_inverse_batched(jd + jo, batch, log2N, tw, st, &nk));
+    ctx->kernel_launches += nk;
+    FCWT_CUDA_TRY(launch_take_real(ctx->adj_g.as<float2>(), N, n, batch, scale, grad_x, st));
+    ctx->kernel_launches += 1;
+    std::vector<double> acc(1 + (size_t)fn);
+    FCWT_CUDA_TRY(cudaMemcpyAsync(acc.data(), ctx->adj_acc.p, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (grad_fb) *grad_fb = scale * acc[0];
+    if (grad_freqs)
+        for (int i = 0; i < fn; i++) grad_freqs[i] = scale * acc[1 + (size_t)i];
+    return FCWT_OK;
 }
 
 int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const char* directory) {

@@ -61,6 +61,9 @@ struct RowDesc {
     long long out_off;  // element offset of the row inside that buffer
     float out_scale;  // 1/N or 1
     int out_row;      // row index inside that buffer (for tensor-map stores)
+    int mode;         // 0: reference mother-table weights; 1: continuous Morlet
+    float ca, cb;     // continuous Morlet: u = ca*q - cb
+    float cnorm;      // continuous Morlet amplitude (the mother table's norm)
 };
 
 enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3, ITEM_PHASE1W = 4 };

@@ -99,7 +99,7 @@ __global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restr
 
 // Batched Stockham pass: blockIdx.y selects the signal. src/dst: 0 = the
 // signal's input (first pass only), 1 = its spectrum X, 2 = its tmp buffer.
-template <int R>
+template <int R, int SIGN>
 __global__ void k_fwd_pass_batched(const FwdJob* __restrict__ jobs, int src_sel, int dst_sel, int log2N, int log2Ns,
                                    const float2* __restrict__ tw) {
     const FwdJob J = jobs[blockIdx.y];
@@ -126,12 +126,12 @@ __global__ void k_fwd_pass_batched(const FwdJob* __restrict__ jobs, int src_sel,
         }
         if (r > 0 && k > 0) {
             float2 w = tw_lookup(tw, log2N, (unsigned)(r * k) << shift);
-            w.y = -w.y;
+            if (SIGN < 0) w.y = -w.y;
             a = cmul(a, w);
         }
         v[r] = a;
     }
-    fft_reg<R, -1>(v);
+    fft_reg<R, SIGN>(v);
     const int base = (j - k) * R + k;
 #pragma unroll
     for (int m = 0; m < R; m++) dst[base + m * Ns] = v[m];
@@ -199,6 +199,10 @@ __device__ bool wait_counter(const unsigned* p, unsigned target, int* err) {
 // row that last wrote bin q into O1; 0 if no row did).
 __device__ __forceinline__ float bin_weight(const RowDesc& R, const float* __restrict__ mother,
                                            const float* __restrict__ pool, float nm1, int q) {
+    if (R.mode == 1) {
+        const float u = R.ca * (float)q - R.cb;
+        return R.cnorm * expf(-0.5f * u * u);
+    }
     float s;
     if (q < R.proc)
         s = R.step;
@@ -722,8 +726,9 @@ cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log
 }
 
 // Forward FFTs of njobs signals of the same padded length 2^log2N.
-cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
-                                   int* n_kernels) {
+template <int SIGN>
+cudaError_t launch_fft_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                               int* n_kernels) {
     *n_kernels = 0;
     if (njobs <= 0) return cudaSuccess;
     if (log2N == 0) return cudaErrorInvalidValue;  // N == 1 is handled by the single-signal path
@@ -746,10 +751,10 @@ cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, con
         const int tb = threads < 256 ? threads : 256;
         dim3 grid((threads + tb - 1) / tb, njobs);
         switch (R) {
-            case 16: dev::k_fwd_pass_batched<16><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
-            case 8: dev::k_fwd_pass_batched<8><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
-            case 4: dev::k_fwd_pass_batched<4><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
-            default: dev::k_fwd_pass_batched<2><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            case 16: dev::k_fwd_pass_batched<16, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            case 8: dev::k_fwd_pass_batched<8, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            case 4: dev::k_fwd_pass_batched<4, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
+            default: dev::k_fwd_pass_batched<2, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2N, log2Ns, tw); break;
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -758,6 +763,17 @@ cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, con
         log2Ns += dev::ilog2c(R);
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                                   int* n_kernels) {
+    return launch_fft_batched<-1>(jobs, njobs, log2N, tw, st, n_kernels);
+}
+
+// Inverse (sign +, unnormalised) batched FFTs, same job layout.
+cudaError_t launch_inverse_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
+                                   int* n_kernels) {
+    return launch_fft_batched<+1>(jobs, njobs, log2N, tw, st, n_kernels);
 }
 
 cudaError_t engine_configure() {

@@ -183,6 +183,10 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
         d.out_off = (long long)r * n;
         d.out_scale = out_scale;
         d.out_row = r;
+        d.mode = (flags & kFlagContinuous) ? 1 : 0;
+        d.ca = rp.ca;
+        d.cb = rp.cb;
+        d.cnorm = host::mother_norm();
     }
     if (!two_phase) {
         const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;

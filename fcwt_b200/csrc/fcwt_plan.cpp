@@ -93,6 +93,45 @@ int plan_signal(int n, bool is_complex, float fb, const float* scales, int fn, i
     const bool avx = (flags & kFlagScalarTrunc) == 0;
     const bool exact = (flags & kFlagExactSupport) != 0;
 
+    if (flags & kFlagContinuous) {
+        // Differentiable Morlet: weight(q) = norm * exp(-u^2/2), u = 2 pi fb (s q / N - 1),
+        // no index rounding, no truncation, no reused bins. Window: |u| <= sqrt(2 ln(1/tau)).
+        const double two_pi = 6.283185307179586;
+        const double umax = exact ? 1e30 : std::sqrt(2.0 * std::log(1.0 / kTrimRel));
+        for (int i = 0; i < fn; i++) {
+            RowPlan& R = out.rows[(size_t)i];
+            const double sc = scales[i];
+            R.ca = (float)(two_pi * fb * sc / N);
+            R.cb = (float)(two_pi * fb);
+            const double qlo = (1.0 - umax / (two_pi * fb)) * N / sc;
+            const double qhi = (1.0 + umax / (two_pi * fb)) * N / sc;
+            int lo = (int)std::max(0.0, std::floor(qlo));
+            int hi = (int)std::min((double)out.half, std::ceil(qhi) + 1.0);
+            if (N < 2) hi = 0;
+            if (hi <= lo) lo = hi = 0;
+            R.proc = hi;
+            R.step = 0.0f;
+            R.lo = lo;
+            R.hi = hi;
+            if (N >= kP2) {
+                const int M = out.M;
+                if (hi <= lo) {
+                    R.K = 1;
+                    R.L = 0;
+                } else {
+                    int L = (lo / kP2) * kP2;
+                    int K = next_pow2((hi - L + kP2 - 1) / kP2);
+                    if (K >= M || (long long)L + (long long)K * kP2 > N) {
+                        K = M;
+                        L = 0;
+                    }
+                    R.K = K;
+                    R.L = L;
+                }
+            }
+        }
+        return 0;
+    }
     for (int i = 0; i < fn; i++) {
         out.rows[(size_t)i].proc = std::min(host::row_proc(N, scales[i], threads, avx), N / 2);
         out.rows[(size_t)i].step = host::row_step(scales[i]);

@@ -11,6 +11,7 @@ namespace fcwt {
 constexpr unsigned kFlagNorm = 1u << 0;
 constexpr unsigned kFlagScalarTrunc = 1u << 1;
 constexpr unsigned kFlagExactSupport = 1u << 2;
+constexpr unsigned kFlagContinuous = 1u << 3;
 
 // Relative weight below which a bin's daughter value is skipped (unless
 // kFlagExactSupport): mother[w] < kTrimRel * max(mother). The skipped terms
@@ -26,6 +27,7 @@ struct RowPlan {
     int lo = 0, hi = 0;  // bins with non-negligible weight: [lo, hi)
     int K = 1;        // phase-1 length
     int L = 0;        // window start
+    float ca = 0, cb = 0;  // continuous Morlet: u = ca*q - cb, weight = norm*exp(-u*u/2)
 };
 
 struct SignalPlan {

@@ -41,6 +41,8 @@ extern "C" {
 #define FCWT_NORM (1u << 0)           /* divide by N: FCWT(..., use_normalization=true) */
 #define FCWT_SCALAR_TRUNC (1u << 1)   /* truncation rule of the reference's non-AVX build */
 #define FCWT_EXACT_SUPPORT (1u << 2)  /* also evaluate bins whose weight is < 2^-36 of the peak */
+#define FCWT_CONTINUOUS (1u << 3)     /* differentiable Morlet: norm*exp(-(2 pi fb (s q/N - 1))^2/2) at every
+                                         bin, no mother-table rounding, truncation or reused bins */
 
 /* ---- output element types */
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
@@ -133,6 +135,19 @@ int fcwt_plan_execute_batched(fcwt_plan* plan, const void* const* inputs, void* 
  * (and any call with different pointers or output type) captures the whole
  * sequence on the context's stream; later calls launch the graph. */
 int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type);
+
+/* ---- differentiable Morlet CWT (FCWT_CONTINUOUS forward)
+ * No reference counterpart (the reference has no gradients). Backward of
+ * y[b,i,t] = c * IFFT_N(FFT_N(x_b) * g_i)[t], g_i(q) = norm*exp(-u^2/2),
+ * u = 2 pi fb (fs/freqs[i] * q/N - 1), c = 1/N with FCWT_NORM, for a batch of
+ * `batch` real signals of n samples and fn rows. Given grad_out = dL/dy*
+ * (complex64 [batch][fn][n], torch convention: dL = Re<grad_out, dy>) it writes
+ * grad_x (float32 [batch][n]) and returns dL/dfb and dL/dfreqs[i] in host
+ * doubles. x, grad_out, grad_x: device pointers; freqs: host array. The input
+ * spectra are recomputed, not stored. */
+int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch, float fb, const float* freqs,
+                             int fn, float fs, unsigned flags, const void* grad_out, float* grad_x, double* grad_fb,
+                             double* grad_freqs);
 
 /* ---- tuning files
  * FCWT::create_FFT_optimization_plan(maxsize, flags), src/fcwt/fcwt.cpp:313-374:

@@ -1,0 +1,110 @@
+"""GPU tests of the differentiable Morlet CWT: forward against a float64
+torch.fft restatement of the same operator, gradients (signal, sigma, centre
+frequencies) against float64 torch autograd of that restatement and against
+float64 central finite differences. Tolerance 1e-4 (relative)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+AMP = math.sqrt(2 * math.pi) * 0.75112554446  # the mother table's amplitude
+
+
+def ref_forward(x, sigma, freqs, fs, norm=True):
+    import torch
+
+    B, n = x.shape
+    N = 1 << int(math.ceil(math.log2(n))) if n > 1 else 1
+    X = torch.fft.fft(x, n=N)
+    q = torch.arange(N // 2, dtype=torch.float64, device=x.device)
+    s = fs / freqs
+    u = 2 * math.pi * sigma * (s[:, None] * q[None, :] / N - 1)
+    g = AMP * torch.exp(-0.5 * u * u)
+    Z = torch.zeros((B, freqs.numel(), N), dtype=torch.complex128, device=x.device)
+    Z[..., : N // 2] = X[:, None, : N // 2] * g[None]
+    y = torch.fft.ifft(Z)
+    if not norm:
+        y = y * N
+    return y[..., :n]
+
+
+def loss_fn(y, target):
+    return ((y.abs() ** 2 - target) ** 2).mean()
+
+
+@pytest.mark.parametrize("n,F,norm", [(1500, 5, True), (5000, 7, False), (20000, 9, True)])
+def test_forward_and_gradients(n, F, norm):
+    import torch
+
+    from fcwt_b200.autograd import morlet_cwt
+
+    rng = np.random.default_rng(n)
+    B, fs = 2, 1000.0
+    t = np.arange(n) / fs
+    x0 = np.stack([np.sin(2 * np.pi * (10 + 30 * t) * t) + 0.1 * rng.standard_normal(n) for _ in range(B)])
+    f0 = np.geomspace(5.0, 150.0, F)
+    sig0 = 2.0
+    target = torch.from_numpy(rng.uniform(0, 0.05, (B, F, n)))
+    if not norm:
+        target = target * (1 << int(math.ceil(math.log2(n)))) ** 2
+
+    # ours
+    x = torch.tensor(x0, dtype=torch.float32, device="cuda", requires_grad=True)
+    sigma = torch.tensor(sig0, dtype=torch.float64, requires_grad=True)
+    freqs = torch.tensor(f0, dtype=torch.float64, requires_grad=True)
+    y = morlet_cwt(x, sigma, freqs, fs, norm)
+    L = loss_fn(y.to(torch.complex128).cpu(), target)
+    L.backward()
+
+    # float64 reference
+    xr = torch.tensor(x0.astype(np.float32).astype(np.float64), requires_grad=True)
+    sr = torch.tensor(sig0, dtype=torch.float64, requires_grad=True)
+    fr = torch.tensor(f0, dtype=torch.float64, requires_grad=True)
+    yr = ref_forward(xr, sr, fr, fs, norm)
+    Lr = loss_fn(yr, target)
+    Lr.backward()
+
+    yd = y.detach().cpu().to(torch.complex128)
+    assert float(torch.linalg.vector_norm(yd - yr.detach()) / torch.linalg.vector_norm(yr.detach())) < 1e-5
+    gx, gxr = x.grad.cpu().double(), xr.grad
+    assert float(torch.linalg.vector_norm(gx - gxr) / torch.linalg.vector_norm(gxr)) < 1e-4
+    assert abs(float(sigma.grad) - float(sr.grad)) <= 1e-4 * abs(float(sr.grad)) + 1e-12
+    gf, gfr = freqs.grad, fr.grad
+    assert float(torch.max(torch.abs(gf - gfr)) / torch.max(torch.abs(gfr))) < 1e-4
+
+    # central finite differences of the float64 operator
+    def L_at(sv, fv):
+        with torch.no_grad():
+            return float(loss_fn(ref_forward(xr.detach(), torch.tensor(sv, dtype=torch.float64),
+                                             torch.tensor(fv, dtype=torch.float64), fs, norm), target))
+    h = 1e-6
+    fd_sig = (L_at(sig0 + h, f0) - L_at(sig0 - h, f0)) / (2 * h)
+    assert abs(float(sigma.grad) - fd_sig) <= 1e-4 * abs(fd_sig) + 1e-10
+    k = F // 2
+    fp, fm = f0.copy(), f0.copy()
+    hf = 1e-6 * f0[k]
+    fp[k] += hf
+    fm[k] -= hf
+    fd_f = (L_at(sig0, fp) - L_at(sig0, fm)) / (2 * hf)
+    assert abs(float(gf[k]) - fd_f) <= 1e-4 * max(abs(fd_f), float(torch.max(torch.abs(gfr)))) + 1e-12
+
+
+def test_learnable_module_trains():
+    import torch
+
+    from fcwt_b200.autograd import LearnableMorletCWT
+
+    n, fs = 4096, 1000.0
+    t = np.arange(n) / fs
+    x = torch.tensor(np.sin(2 * np.pi * 40 * t), dtype=torch.float32, device="cuda").reshape(1, n)
+    layer = LearnableMorletCWT([30.0, 55.0], fs, sigma=2.0)
+    y = layer(x)
+    e0 = float((y.detach().abs() ** 2).mean())
+    (-(y.abs() ** 2).mean()).backward()
+    # moving the centre frequencies toward 40 Hz increases the energy
+    assert float(layer.freqs.grad[0]) < 0 < float(layer.freqs.grad[1])
+    assert e0 > 0 and layer.sigma.grad is not None and torch.isfinite(layer.sigma.grad)
