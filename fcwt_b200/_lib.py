@@ -29,6 +29,10 @@ FCWT_OUT_C64 = 0
 FCWT_OUT_BF16 = 1
 FCWT_OUT_F16 = 2
 
+FCWT_ENGINE_AUTO = 0
+FCWT_ENGINE_CUDA_CORES = 1
+FCWT_ENGINE_TENSOR_CORES = 2
+
 # Every symbol include/fcwt_b200.h declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -41,6 +45,7 @@ SIGNATURES = {
     "fcwt_context_destroy": (_i, [_vp]),
     "fcwt_context_set_stream": (_i, [_vp, _vp]),
     "fcwt_synchronize": (_i, [_vp]),
+    "fcwt_context_set_engine": (_i, [_vp, _i]),
     "fcwt_profile_enable": (_i, [_vp, _i]),
     "fcwt_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fcwt_find2power": (_i, [_i]),
@@ -145,6 +150,11 @@ class Context:
 
     def synchronize(self) -> None:
         call("fcwt_synchronize", self.handle)
+
+    def set_engine(self, mode: int) -> None:
+        """FCWT_ENGINE_AUTO, FCWT_ENGINE_CUDA_CORES or FCWT_ENGINE_TENSOR_CORES
+        for plans built afterwards (drops this context's plan cache)."""
+        call("fcwt_context_set_engine", self.handle, int(mode))
 
     def profile_enable(self, enable: bool = True) -> None:
         call("fcwt_profile_enable", self.handle, 1 if enable else 0)

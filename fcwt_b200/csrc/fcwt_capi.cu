@@ -38,6 +38,8 @@ cudaError_t engine_configure();
 cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
 cudaError_t launch_engine(const EngineParams& p, const CUtensorMap& omap, int grid, cudaStream_t st);
+cudaError_t tc_configure();
+cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st);
 }  // namespace fcwt
 
 namespace {
@@ -146,6 +148,7 @@ struct fcwt_context {
     cudaStream_t stream = nullptr;
     int num_sms = 0;
     int engine_ctas = 0;  // persistent grid of the row engine
+    int engine_mode = FCWT_ENGINE_AUTO;  // which rows the tensor-core engine takes
     DevBuf in_stage, out_stage, tmp, scratch, counters, err;
     int* err_host = nullptr;  // pinned mirror of the device error word
     TuneChoice tune[fcwt::kMaxLog2N + 1];
@@ -191,10 +194,11 @@ struct fcwt_plan {
     bool is_complex = false;
     std::vector<PlanSignal> sig;
     std::vector<PlanTables> tables;
-    DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs;
+    DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs, tc_rows;
     fcwt::FwdJob* jobs_host = nullptr;  // pinned staging of the batched forward jobs
     int n_items = 0;
     int n_rows = 0;
+    int n_tc = 0;  // rows run by the tensor-core engine
     int slots = 0;
     long long slot_elems = 0;
     bool two_phase = false;
@@ -227,6 +231,7 @@ void plan_free(fcwt_plan* p) {
     p->fwd_jobs.release();
     p->fwd_tmp.release();
     p->graph_jobs.release();
+    p->tc_rows.release();
     if (p->jobs_host) cudaFreeHost(p->jobs_host);
     delete p;
 }
@@ -256,6 +261,7 @@ int plan_build(fcwt_plan* P) {
     std::vector<float> pool;
     std::vector<RowDesc> rows;
     std::vector<int> two_phase_rows;  // global indices, in order
+    std::vector<int> tc_rows;         // rows of the tensor-core engine, in order
     std::vector<Item> items;
     int max_two_phase_log2N = 0;
     for (int s = 0; s < nsig; s++) {
@@ -288,9 +294,21 @@ int plan_build(fcwt_plan* P) {
             d.ca = rp.ca;
             d.cb = rp.cb;
             d.cnorm = host::mother_norm();
+            d.kp = 0;
             const int g = (int)rows.size();
+            // tensor-core rows: window [L, L + 1024 kp), L a multiple of 1024, kp <= 16
+            int tc_kp = 0;
+            if (ctx->engine_mode != FCWT_ENGINE_CUDA_CORES && sp.N >= kTcMinN) {
+                const int L = rp.hi > rp.lo ? (rp.lo / kP2) * kP2 : 0;
+                const int kw = rp.hi > rp.lo ? (rp.hi - L + kP2 - 1) / kP2 : 0;
+                if (kw <= kTcMaxKp) tc_kp = kw <= 8 ? 8 : 16;
+                if (tc_kp) d.L = L;
+            }
+            d.kp = tc_kp;
             rows.push_back(d);
-            if (sp.N > kMaxFusedN) {
+            if (tc_kp) {
+                tc_rows.push_back(g);
+            } else if (sp.N > kMaxFusedN) {
                 two_phase_rows.push_back(g);
                 max_two_phase_log2N = std::max(max_two_phase_log2N, sp.log2N);
             } else {
@@ -335,6 +353,7 @@ int plan_build(fcwt_plan* P) {
         P->slot_elems = slot_elems;
     }
     P->n_items = (int)items.size();
+    P->n_tc = (int)tc_rows.size();
 
     // device buffers and tables
     for (auto& T : P->tables) {
@@ -373,6 +392,11 @@ int plan_build(fcwt_plan* P) {
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->rows.p, rows.data(), rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
     if (!items.empty())
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->items.p, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice, st));
+    if (!tc_rows.empty()) {
+        FCWT_CUDA_TRY(P->tc_rows.ensure(tc_rows.size() * sizeof(int)));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->tc_rows.p, tc_rows.data(), tc_rows.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, st));
+    }
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;
 }
@@ -453,7 +477,8 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
             off += g.second;
         }
     }
-    const size_t n_counters = 1 + 2 * (size_t)P->n_rows;
+    // [0]: item queue; a_done[rows]; b_done[rows]; tensor-core row queue
+    const size_t n_counters = 2 + 2 * (size_t)P->n_rows;
     FCWT_CUDA_TRY(ctx->counters.ensure(n_counters * sizeof(unsigned)));
     FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, n_counters * sizeof(unsigned), st));
     FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
@@ -476,11 +501,12 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     ep.err = ctx->err.as<int>();
     CUtensorMap omap;
     std::memset(&omap, 0, sizeof(omap));
-    if (nsig == 1) {
+    int map_ok = 0;
+    if (nsig == 1 && out_type == FCWT_OUT_C64 && (P->two_phase || P->n_tc > 0)) {
         const PlanSignal& S = P->sig[0];
-        ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64 &&
-                        encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap)) ? 1 : 0;
+        map_ok = encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
     }
+    ep.tma_store = P->two_phase ? map_ok : 0;
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     const bool prof = ctx->profiling && allow_profiling;
@@ -494,8 +520,25 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         }
         FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
     }
-    FCWT_CUDA_TRY(launch_engine(ep, omap, grid, st));
-    ctx->kernel_launches += 1;
+    if (P->n_tc > 0) {
+        TcParams tp;
+        std::memset(&tp, 0, sizeof(tp));
+        tp.sigs = ep.sigs;
+        tp.rows = ep.rows;
+        tp.row_list = P->tc_rows.as<int>();
+        tp.n_list = P->n_tc;
+        tp.stale_pool = ep.stale_pool;
+        tp.counter = ctx->counters.as<unsigned>() + n_counters - 1;
+        for (int s = 0; s < nsig; s++) tp.outs[s] = dout[s];
+        tp.err = ep.err;
+        tp.tma_store = map_ok;
+        FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_tc, ctx->num_sms)), st));
+        ctx->kernel_launches += 1;
+    }
+    if (P->n_items > 0) {
+        FCWT_CUDA_TRY(launch_engine(ep, omap, grid, st));
+        ctx->kernel_launches += 1;
+    }
     if (prof) {
         FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
         ctx->ev_used.push_back(ev);
@@ -659,6 +702,7 @@ int fcwt_context_create(int device, fcwt_context** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&c->err_host, sizeof(int));
     if (e == cudaSuccess) e = fcwt::engine_configure();
+    if (e == cudaSuccess) e = fcwt::tc_configure();
     int per_sm = 0;
     if (e == cudaSuccess) e = fcwt::engine_blocks_per_sm(&per_sm);
     c->engine_ctas = std::max(1, per_sm) * c->num_sms;
@@ -707,6 +751,21 @@ int fcwt_context_destroy(fcwt_context* ctx) {
 int fcwt_context_set_stream(fcwt_context* ctx, void* stream) {
     if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+    return FCWT_OK;
+}
+
+int fcwt_context_set_engine(fcwt_context* ctx, int mode) {
+    if (!ctx) return fail(FCWT_ERR_INVALID, "null context");
+    if (mode != FCWT_ENGINE_AUTO && mode != FCWT_ENGINE_CUDA_CORES && mode != FCWT_ENGINE_TENSOR_CORES)
+        return fail(FCWT_ERR_INVALID, "unknown engine mode");
+    if (mode != ctx->engine_mode) {
+        // cached plans were built for the previous mode
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& e : ctx->cache) plan_free(e.plan);
+        ctx->cache.clear();
+        ctx->engine_mode = mode;
+    }
     return FCWT_OK;
 }
 

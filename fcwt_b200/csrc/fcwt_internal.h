@@ -64,6 +64,7 @@ struct RowDesc {
     int mode;         // 0: reference mother-table weights; 1: continuous Morlet
     float ca, cb;     // continuous Morlet: u = ca*q - cb
     float cnorm;      // continuous Morlet amplitude (the mother table's norm)
+    int kp;           // tensor-core rows: 1024-bin blocks of the window, padded to 8 or 16
 };
 
 enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3, ITEM_PHASE1W = 4 };
@@ -107,6 +108,23 @@ struct EngineParams {
     int out_type;
     int* err;                  // device error word (0 = ok)
     int tma_store;             // phase-2 outputs via the tensor map (buffer 0, complex64, even n)
+};
+
+// Tensor-core row engine (fcwt_tc.cu): rows whose window [L, L + 1024 kp)
+// (L a multiple of 1024) spans at most kTcMaxKp blocks, for N >= kTcMinN.
+constexpr int kTcMaxKp = 16;
+constexpr int kTcMinN = 16384;
+
+struct TcParams {
+    const SigDesc* sigs;
+    const RowDesc* rows;
+    const int* row_list;       // rows of this launch, in queue order
+    int n_list;
+    const float* stale_pool;
+    unsigned* counter;         // row queue head
+    void* outs[kMaxOuts];
+    int* err;
+    int tma_store;             // outputs via the tensor map (buffer 0, complex64, even n)
 };
 
 // Error bits written by device code into EngineParams::err.

@@ -1,0 +1,459 @@
+// Tensor-core row engine (sm_100a: tcgen05 MMA with tensor-memory operands).
+//
+// Same transform as the CUDA-core engine (fcwt_kernels.cu): the daughter
+// product of the reference (src/fcwt/fcwt.cpp:197-311), the inverse FFT
+// (fcwt.cpp:418-429), the normalisation (fcwt.cpp:431-445) and the crop to n
+// (fcwt.cpp:396-416). With t = c + M a and q = L + k2 + 1024 k1 (L a multiple
+// of 1024, k2 < 1024, k1 < Kp), the four-step inverse transform of a row is
+//     G[c][k2]   = w_N^{k2 c} * sum_{k1 < Kp} Z[L + k2 + 1024 k1] * B[k1][c],
+//     B[k1][c]   = w_M^{k1 c} * w_N^{L c},
+//     y[c + M a] = DFT_1024(G[c][.])[a],
+// (w_X = exp(+2 pi i / X), Z = spectrum x daughter weights x 1/N). For rows
+// whose window spans at most 16 blocks of 1024 bins, the first line is a
+// complex GEMM [1024 k2 x Kp] x [Kp x M] with a short inner dimension; this
+// engine runs it on the tensor cores in split FP16 (hi + lo, three products,
+// FP32 accumulation: about 2^-21 relative error per element), so phase 1
+// costs no FFT work and no scratch round trip through L2.
+//
+// One persistent CTA of 16 warps per SM takes rows from a queue. Per row:
+//   pre-pass  all warps evaluate Z on the window, scale it by 2^e
+//             (max |Z| 2^e in [2^14, 2^15)), split it into FP16 hi + lo and
+//             store it in tensor memory as the A operand: tile t (k2 in
+//             [128 t, 128 t + 128)) is lanes 0..127, columns
+//             [(2t + p) Kp, +Kp) for p = hi, lo; column k1 holds (re, im) as a
+//             half2, i.e. GEMM K index 2 k1 + {0, 1}.
+//   groups    the two halves of the CTA (8 warps each) take alternating groups
+//             of 8 columns c. Per group: B (16 x 2Kp, K-major, FP16 hi + lo)
+//             in SMEM, rows 0..7 giving Re G and rows 8..15 Im G of the 8
+//             columns; 24 or 48 MMAs (M=128, N=16, K=16; hi*hi + lo*hi +
+//             hi*lo) into the half's accumulator columns, completion signalled
+//             on an mbarrier; drain (tcgen05.ld), twiddle w_N^{k2 c} 2^-e, SMEM
+//             column tiles; one warp per column runs the 1024-point DFT;
+//             swizzled staging and TMA tensor stores of [256 a][8 c] boxes.
+//             The MMAs of the half's next group are issued before its DFT.
+// Tensor memory: 512 columns per CTA (A: 0..255, accumulators of half h:
+// 256 + 128 h + 16 t for tile t).
+#include "fcwt_dev.cuh"
+
+namespace fcwt {
+namespace dev {
+
+constexpr int kTcThreads = 512;
+constexpr int kTcCols = 8;          // columns per group (one per warp of a half)
+constexpr int kTcTmemCols = 512;
+constexpr int kTcDcol = 256;        // first accumulator column
+constexpr int kTcTwhiSmem = 512;    // w_M table kept in SMEM when M <= this
+constexpr int kTcGbufBytes = kTcCols * kP2 * 8;   // 64 KB: G tiles / output staging of one half
+constexpr int kTcOffTwlo = 2 * kTcGbufBytes;
+constexpr int kTcOffT2 = kTcOffTwlo + kP2 * 8;
+constexpr int kTcOffTwhi = kTcOffT2 + kP2 * 8;
+constexpr int kTcOffB = kTcOffTwhi + kTcTwhiSmem * 8;
+constexpr int kTcBBytes = 16 * 2 * kTcMaxKp * 2;  // one B operand (16 rows x 2Kp halves), 1 KB
+constexpr int kTcOffEnd = kTcOffB + 2 * 2 * kTcBBytes;
+constexpr size_t kTcSmemBytes = (size_t)kTcOffEnd + 1024;
+static_assert(4 * kBoxBytes == kTcGbufBytes, "staging boxes fill one G buffer");
+
+// Instruction descriptor: D f32, A/B f16, both K-major, N = 16, M = 128.
+constexpr uint32_t kTcIdesc = (1u << 4) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor, K-major without swizzle: core matrices of
+// 8 rows x 16 bytes; lbo = byte distance between core matrices along K, sbo =
+// between 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+        "r"(a), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier (gives up after
+// kWaitLimitNs, recording kErrWaitTimeout).
+__device__ bool mbar_wait(uint32_t mbar, uint32_t parity, int* err) {
+    unsigned long long t0 = 0;
+    for (unsigned it = 0;; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (it == 0) {
+            t0 = global_ns();
+        } else if ((it & 63u) == 0 && global_ns() - t0 > kWaitLimitNs) {
+            atomicOr(err, kErrWaitTimeout);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void half_bar(int h) { asm volatile("bar.sync %0, 256;" ::"r"(1 + h) : "memory"); }
+
+__device__ __forceinline__ uint32_t h2bits(__half2 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// Warp-level 1024-point DFT (sign +) with an XOR-swizzled 32 x 32 transpose
+// buffer (8 KB): on entry lane l holds x[m] = G[l + 32 m]; on exit lane l
+// holds x[h] = Y[l + 32 h].
+__device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, float2* __restrict__ tb,
+                                                 const float2* __restrict__ t2) {
+    fft_reg<32, +1>(x);
+#pragma unroll
+    for (int a = 1; a < 32; a++) x[a] = cmul(x[a], t2[a * 32 + lane]);
+#pragma unroll
+    for (int a = 0; a < 32; a++) tb[a * 32 + (lane ^ a)] = x[a];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) x[k] = tb[lane * 32 + (k ^ lane)];
+    __syncwarp();
+    fft_reg<32, +1>(x);
+}
+
+// B operand of group g: rows j (Re G) and 8 + j (Im G) of column c = 8 g + j,
+// K index 2 k1 + {re, im}; byte offset of element (n, k) in the canonical
+// K-major layout: (k / 16) * 512 + (n / 8) * 256 + ((k / 8) % 2) * 128 +
+// (n % 8) * 16 + (k % 8) * 2.
+template <int KP>
+__device__ __forceinline__ void build_b(int g, int ht, int M, unsigned Nm, int L, const float2* __restrict__ twlo,
+                                        const float2* __restrict__ twhi, unsigned char* bhi, unsigned char* blo) {
+    if (ht < kTcCols * KP) {
+        const int j = ht / KP;
+        const int k1 = ht - j * KP;
+        const int c = g * kTcCols + j;
+        const float2 w = cmul(twhi[(unsigned)(k1 * c) & (unsigned)(M - 1)],
+                              tw_n(twlo, twhi, ((unsigned)L * (unsigned)c) & Nm));
+        const int k = 2 * k1;
+        const int off0 = (k >> 4) * 512 + ((k >> 3) & 1) * 128 + j * 16 + (k & 7) * 2;  // row j
+        const int off1 = off0 + 256;                                                     // row 8 + j
+        const __half2 h0 = __floats2half2_rn(w.x, -w.y);
+        const __half2 h1 = __floats2half2_rn(w.y, w.x);
+        const float2 f0 = __half22float2(h0);
+        const float2 f1 = __half22float2(h1);
+        *reinterpret_cast<__half2*>(bhi + off0) = h0;
+        *reinterpret_cast<__half2*>(bhi + off1) = h1;
+        *reinterpret_cast<__half2*>(blo + off0) = __floats2half2_rn(w.x - f0.x, -w.y - f0.y);
+        *reinterpret_cast<__half2*>(blo + off1) = __floats2half2_rn(w.y - f1.x, w.x - f1.y);
+    }
+}
+
+// The MMAs of one group: for each k2 tile, D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
+template <int KP>
+__device__ __forceinline__ void issue_group(uint32_t tmem, uint32_t dcol, uint32_t bhi, uint32_t blo) {
+#pragma unroll 1
+    for (int t = 0; t < 8; t++) {
+        const uint32_t d = dcol + 16u * t;
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+            const uint32_t a = tmem + (uint32_t)((2 * t + (p == 1 ? 1 : 0)) * KP);
+            const uint32_t b = p == 2 ? blo : bhi;
+#pragma unroll
+            for (int kb = 0; kb < KP / 8; kb++)
+                mma_ts(d, a + 8u * kb, umma_desc(b + 512u * kb, 128, 256), (p | kb) != 0 ? 1u : 0u);
+        }
+    }
+}
+
+template <int KP, int OT>
+__device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
+                                       const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
+                                       const float2* __restrict__ twhi, const float2* __restrict__ t2, uint32_t tmem,
+                                       uint32_t mbar_h, uint32_t& phase, float* s_red) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int h = warp >> 3;
+    const int ht = tid & 255;
+    const int wl = warp & 7;
+    const int qd = warp & 3;
+    const int log2N = S.log2N;
+    const int N = 1 << log2N;
+    const int M = N >> kLog2P2;
+    const unsigned Nm = (unsigned)N - 1u;
+    const int n = S.n;
+    const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+
+    // ---- pre-pass: Z on the window into tensor memory (split FP16)
+    float scale, inv;
+    {
+        const float nm1 = (float)N - 1.0f;
+        const int tsel = warp >> 2;  // this warp's tiles: tsel, tsel + 4
+        float2 z[2][KP];
+        float mx = 0.0f;
+#pragma unroll
+        for (int ti = 0; ti < 2; ti++) {
+            const int k2 = 128 * (tsel + 4 * ti) + 32 * qd + lane;
+#pragma unroll
+            for (int k1 = 0; k1 < KP; k1++) {
+                const float2 v = bin_value(R, S, P.stale_pool, nm1, R.L + k2 + kP2 * k1);
+                z[ti][k1] = v;
+                mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) s_red[warp] = mx;
+        __syncthreads();
+        mx = 0.0f;
+#pragma unroll
+        for (int w = 0; w < kTcThreads / 32; w++) mx = fmaxf(mx, s_red[w]);
+        int ex = 0;
+        if (mx > 0.0f) frexpf(mx, &ex);
+        const int e2 = max(-126, min(126, 15 - ex));
+        scale = ldexpf(1.0f, e2);
+        inv = ldexpf(1.0f, -e2);
+#pragma unroll
+        for (int ti = 0; ti < 2; ti++) {
+            const int t = tsel + 4 * ti;
+            uint32_t hv[KP], lv[KP];
+#pragma unroll
+            for (int k1 = 0; k1 < KP; k1++) {
+                const float a = z[ti][k1].x * scale;
+                const float b = z[ti][k1].y * scale;
+                const __half2 hh = __floats2half2_rn(a, b);
+                const float2 hf = __half22float2(hh);
+                hv[k1] = h2bits(hh);
+                lv[k1] = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+            }
+            const uint32_t ta = tmem + lane_base + (uint32_t)(2 * t * KP);
+#pragma unroll
+            for (int q = 0; q < KP / 8; q++) {
+                tmem_st8(ta + 8u * q, hv + 8 * q);
+                tmem_st8(ta + KP + 8u * q, lv + 8 * q);
+            }
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+
+    // ---- column groups
+    const int ng = M / kTcCols;
+    float2* gbuf = reinterpret_cast<float2*>(sm + h * kTcGbufBytes);
+    unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
+    unsigned char* blo = bhi + kTcBBytes;
+    const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
+    const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
+    const bool tma = P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0;
+    void* outb = P.outs[R.out_buf];
+    int g = h;
+    if (g < ng) {
+        build_b<KP>(g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        fence_proxy_async_smem();
+        half_bar(h);
+        if (ht == 0) {
+            tc_fence_after();
+            issue_group<KP>(tmem, dcol, bhi_a, blo_a);
+            mma_commit(mbar_h);
+        }
+    }
+    const int tb = (wl >> 2) * 4;  // this warp drains tiles tb .. tb + 3
+    while (g < ng) {
+        mbar_wait(mbar_h, phase, P.err);
+        phase ^= 1u;
+        tc_fence_after();
+        const int c0 = g * kTcCols;
+        float2 gv[4][kTcCols];
+#pragma unroll
+        for (int tt = 0; tt < 4; tt++) {
+            uint32_t r[16];
+            tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
+            tmem_wait_ld();
+            const int k2 = 128 * (tb + tt) + 32 * qd + lane;
+            float2 w = cscale(tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)c0) & Nm), inv);
+            const float2 stp = twlo[k2];
+#pragma unroll
+            for (int j = 0; j < kTcCols; j++) {
+                gv[tt][j] = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
+                if (j + 1 < kTcCols) w = cmul(w, stp);
+            }
+        }
+        tc_fence_before();
+        if (tma && ht == 0) bulk_wait_read_all();
+        half_bar(h);  // accumulators drained; the G buffer is free
+        const int gn = g + 2;
+        if (gn < ng) build_b<KP>(gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+#pragma unroll
+        for (int tt = 0; tt < 4; tt++) {
+            const int k2 = 128 * (tb + tt) + 32 * qd + lane;
+#pragma unroll
+            for (int j = 0; j < kTcCols; j++) gbuf[j * kP2 + k2] = gv[tt][j];
+        }
+        fence_proxy_async_smem();
+        half_bar(h);  // G tiles and the next B in SMEM
+        if (ht == 0 && gn < ng) {
+            tc_fence_after();
+            issue_group<KP>(tmem, dcol, bhi_a, blo_a);
+            mma_commit(mbar_h);
+        }
+        // phase 2: one column per warp
+        float2* col = gbuf + wl * kP2;
+        float2 x[32];
+#pragma unroll
+        for (int m = 0; m < 32; m++) x[m] = col[lane + 32 * m];
+        __syncwarp();
+        dft1024_warp_xor(x, lane, col, t2);
+        half_bar(h);  // every column is in registers
+        unsigned char* stage = reinterpret_cast<unsigned char*>(gbuf);
+#pragma unroll
+        for (int hh = 0; hh < 32; hh++) *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * hh, wl)) = x[hh];
+        const long long row0 = R.out_off + c0;
+        if (tma) {
+            fence_proxy_async_smem();
+            half_bar(h);
+            const int n_full = n / M;
+            if (ht == 0) {
+                for (int j = 0; j < 4 && j * kBoxRows < n_full; j++)
+                    tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, R.out_row);
+                bulk_commit();
+            }
+            const int tail = n - n_full * M;
+            if (ht < kTcCols && c0 + ht < tail && n_full < kP2)
+                store_out<OT>(outb, row0 + ht + (long long)M * n_full,
+                              *reinterpret_cast<const float2*>(stage + stage_off(n_full, ht)));
+        } else {
+            half_bar(h);
+            for (int idx = ht; idx < kTcCols * kP2; idx += 256) {
+                const int w = idx & (kTcCols - 1);
+                const int a = idx >> 3;
+                if (c0 + w + (long long)M * a < n)
+                    store_out<OT>(outb, row0 + w + (long long)M * a,
+                                  *reinterpret_cast<const float2*>(stage + stage_off(a, w)));
+            }
+        }
+        g = gn;
+    }
+}
+
+template <int OT>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_row_tc(const __grid_constant__ TcParams P, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    unsigned char* sm = tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u);
+    float2* twlo = reinterpret_cast<float2*>(sm + kTcOffTwlo);
+    float2* t2 = reinterpret_cast<float2*>(sm + kTcOffT2);
+    float2* twhi_s = reinterpret_cast<float2*>(sm + kTcOffTwhi);
+    __shared__ __align__(8) unsigned long long s_mbar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_idx;
+    __shared__ int s_log2N;
+    __shared__ RowDesc s_R;
+    __shared__ SigDesc s_S;
+    __shared__ float s_red[kTcThreads / 32];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int h = warp >> 3;
+
+    for (int j = tid; j < kP2; j += kTcThreads) {
+        const int a = j >> 5, l = j & 31;
+        double s, c;
+        sincospi(2.0 * (double)((a * l) & 1023) / 1024.0, &s, &c);
+        t2[j] = make_float2((float)c, (float)s);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_log2N = -1;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t mbar_h = smem_u32(&s_mbar[h]);
+    uint32_t phase = 0;
+
+    for (;;) {
+        if (tid == 0) {
+            const int i = (int)atomicAdd(P.counter, 1u);
+            s_idx = i;
+            if (i < P.n_list) {
+                s_R = P.rows[P.row_list[i]];
+                s_S = P.sigs[s_R.sig];
+            }
+        }
+        __syncthreads();
+        if (s_idx >= P.n_list) break;
+        const int log2N = s_S.log2N;
+        const int M = 1 << (log2N - kLog2P2);
+        if (log2N != s_log2N) {
+            for (int j = tid; j < kP2; j += kTcThreads) twlo[j] = s_S.tw[j];
+            if (M <= kTcTwhiSmem)
+                for (int j = tid; j < M; j += kTcThreads) twhi_s[j] = s_S.tw[kP2 + j];
+        }
+        __syncthreads();
+        if (tid == 0) s_log2N = log2N;
+        const float2* twhi = M <= kTcTwhiSmem ? twhi_s : s_S.tw + kP2;
+        if (s_R.kp > 8)
+            row_tc<16, OT>(P, &omap, s_R, s_S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red);
+        else
+            row_tc<8, OT>(P, &omap, s_R, s_S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red);
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if ((tid & 255) == 0 && P.tma_store) bulk_wait_all();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+}
+
+}  // namespace dev
+
+size_t tc_smem_bytes() { return dev::kTcSmemBytes; }
+
+cudaError_t tc_configure() {
+    cudaError_t e = cudaFuncSetAttribute(dev::k_row_tc<OUT_C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dev::kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(dev::k_row_tc<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dev::kTcSmemBytes);
+}
+
+cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st) {
+    switch (out_type) {
+        case OUT_BF16: dev::k_row_tc<OUT_BF16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_F16: dev::k_row_tc<OUT_F16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        default: dev::k_row_tc<OUT_C64><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace fcwt

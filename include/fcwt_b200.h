@@ -65,6 +65,18 @@ int fcwt_context_set_stream(fcwt_context* ctx, void* cuda_stream);
 /* Wait for all work of the context and report device-side errors. */
 int fcwt_synchronize(fcwt_context* ctx);
 
+/* Row engine selection (no reference counterpart: the reference has one CPU
+ * path). FCWT_ENGINE_AUTO and FCWT_ENGINE_TENSOR_CORES run every row whose bin
+ * window spans at most 16 blocks of 1024 bins (N >= 16384) on the tcgen05
+ * tensor-core engine and the other rows on the CUDA-core engine;
+ * FCWT_ENGINE_CUDA_CORES runs every row on the CUDA-core engine. Changing the
+ * mode drops the context's cached plans; plans created earlier keep the mode
+ * they were built with. */
+#define FCWT_ENGINE_AUTO 0
+#define FCWT_ENGINE_CUDA_CORES 1
+#define FCWT_ENGINE_TENSOR_CORES 2
+int fcwt_context_set_engine(fcwt_context* ctx, int mode);
+
 /* Profiling: when enabled, every transform of the context records CUDA events
  * around its row-engine launch (on the context's stream). */
 int fcwt_profile_enable(fcwt_context* ctx, int enable);

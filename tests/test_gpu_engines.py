@@ -1,0 +1,152 @@
+"""The two row engines on the same inputs: the tcgen05 tensor-core engine
+(split-FP16 phase-1 GEMM, rows whose window spans <= 16 blocks of 1024 bins,
+N >= 16384) and the CUDA-core engine. Both against the float64 oracle at
+rel-L2 <= 1e-5 (complex64) and <= 3e-3 (16-bit outputs), and against each
+other. Cases cover the reference's stale bins (sigma 0.5), norm off, complex
+input, odd n, several signals in one plan (plain stores instead of tensor-map
+stores) and the continuous Morlet of the differentiable operator."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.oracle import LINFREQS, LOGSCALES, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture
+def ctx(fcwt):
+    from fcwt_b200 import _lib
+
+    c = _lib.context(0)
+    yield c
+    c.set_engine(_lib.FCWT_ENGINE_AUTO)
+
+
+def _tc_rows(fcwt, n, sc, fb, T, exact=False):
+    """Rows the tensor-core engine takes (host-side rule of the planner)."""
+    _, lo, hi = fcwt.row_truncation(n, sc, threads=T, exact_support=exact, fb=fb)
+    N = 1 << int(np.ceil(np.log2(n)))
+    if N < 16384:
+        return np.zeros(len(sc), bool)
+    L = np.where(hi > lo, (lo // 1024) * 1024, 0)
+    kw = np.where(hi > lo, (hi - L + 1023) // 1024, 0)
+    return kw <= 16
+
+
+def _plan_run(fcwt, ctx, mode, x, sc, fb, T, norm, complex_input=False, out_type=0):
+    ctx.set_engine(mode)
+    p = fcwt.Plan(x.size, sc, fb=fb, threads=T, norm=norm, complex_input=complex_input)
+    if out_type == 0:
+        out = np.zeros((len(sc), x.size), np.complex64)
+    else:
+        out = np.zeros((len(sc), x.size, 2), np.uint16)
+    p.execute(x, out, out_type=out_type)
+    p.close()
+    return out
+
+
+def _to_complex(out16, out_type):
+    import torch
+
+    t = torch.from_numpy(out16.view(np.int16))
+    f = t.view(torch.bfloat16 if out_type == 1 else torch.float16).float().numpy()
+    return f[..., 0] + 1j * f[..., 1]
+
+
+CASES = [
+    # n, fb, scaletype, fs, f0, f1, fn, threads, norm
+    (100000, 2.0, LINFREQS, 1000, 1.0, 101.0, 64, 1, True),
+    (16384, 2.0, LOGSCALES, 1000, 2.0, 200.0, 64, 8, True),
+    (30000, 0.5, LOGSCALES, 1000, 2.0, 300.0, 48, 2, False),
+    (65536, 6.0, LINFREQS, 30000, 1.0, 5000.0, 40, 8, True),
+    (54321, 4.0, LOGSCALES, 200000, 10.0, 80000.0, 40, 1, True),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"n{c[0]}_fb{c[1]}_T{c[7]}")
+def test_engines_match_oracle(fcwt, oracle, ctx, case):
+    from fcwt_b200 import _lib
+
+    n, fb, st, fs, f0, f1, fn, T, norm = case
+    rng = np.random.default_rng(n + fn)
+    x = (rng.standard_normal(n) + 2 * np.sin(np.arange(n) * 0.01)).astype(np.float32)
+    sc = oracle.scales(st, fs, f0, f1, fn)
+    assert _tc_rows(fcwt, n, sc, fb, T).any()
+    ref = oracle.cwt_fp64(x, sc, fb, T, norm)
+    tc = _plan_run(fcwt, ctx, _lib.FCWT_ENGINE_TENSOR_CORES, x, sc, fb, T, norm)
+    cc = _plan_run(fcwt, ctx, _lib.FCWT_ENGINE_CUDA_CORES, x, sc, fb, T, norm)
+    assert rel_l2(tc, ref) < TOL
+    assert rel_l2(cc, ref) < TOL
+    assert rel_l2(tc, cc) < 2 * TOL
+    # row by row, for rows carrying energy
+    e = np.linalg.norm(ref, axis=1)
+    for i in np.nonzero(e > 1e-3 * e.max())[0]:
+        assert rel_l2(tc[i], ref[i]) < 4 * TOL
+
+
+def test_tensor_engine_complex_input_odd_n(fcwt, oracle, ctx):
+    from fcwt_b200 import _lib
+
+    n = 40001
+    rng = np.random.default_rng(7)
+    x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    sc = oracle.scales(LOGSCALES, 1000, 1.0, 450.0, 36)
+    tc = _plan_run(fcwt, ctx, _lib.FCWT_ENGINE_TENSOR_CORES, x, sc, 2.0, 4, True, complex_input=True)
+    ref = oracle.cwt_fp64(x, sc, 2.0, 4, True)
+    assert rel_l2(tc, ref) < TOL
+
+
+@pytest.mark.parametrize("out_type", [1, 2], ids=["bf16", "f16"])
+def test_tensor_engine_16bit_outputs(fcwt, oracle, ctx, out_type):
+    from fcwt_b200 import _lib
+
+    n = 100000
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(n).astype(np.float32)
+    sc = oracle.scales(LINFREQS, 1000, 1.0, 101.0, 32)
+    out = _plan_run(fcwt, ctx, _lib.FCWT_ENGINE_TENSOR_CORES, x, sc, 2.0, 1, True, out_type=out_type)
+    ref = oracle.cwt_fp64(x, sc, 2.0, 1, True)
+    assert rel_l2(_to_complex(out, out_type), ref) < 3e-3
+
+
+def test_tensor_engine_batched_plan(fcwt, oracle, ctx):
+    """Several signals of different lengths and grids in one plan (the
+    tensor-core engine stores through SMEM staging, no tensor map)."""
+    from fcwt_b200 import _lib
+
+    ctx.set_engine(_lib.FCWT_ENGINE_TENSOR_CORES)
+    rng = np.random.default_rng(11)
+    ns = [20000, 70000, 16385]
+    grids = [oracle.scales(LOGSCALES, 30000, 1.0, 5000.0, k) for k in (24, 40, 16)]
+    xs = [rng.standard_normal(n).astype(np.float32) for n in ns]
+    bp = fcwt.BatchPlan(ns, grids, fb=6.0, threads=1, norm=True)
+    outs = [np.zeros((len(g), n), np.complex64) for g, n in zip(grids, ns)]
+    bp.execute(xs, outs)
+    bp.close()
+    for x, g, o in zip(xs, grids, outs):
+        assert rel_l2(o, oracle.cwt_fp64(x, g, 6.0, 1, True)) < TOL
+
+
+def test_tensor_engine_device_tensors_repeat(fcwt, oracle, ctx):
+    """Device-resident input and output, several executions of one plan."""
+    import torch
+    from fcwt_b200 import _lib
+
+    ctx.set_engine(_lib.FCWT_ENGINE_TENSOR_CORES)
+    n = 100000
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(n).astype(np.float32)
+    sc = oracle.scales(LINFREQS, 1000, 1.0, 101.0, 300)
+    p = fcwt.Plan(n, sc, fb=2.0, threads=1, norm=True)
+    xd = torch.from_numpy(x).cuda()
+    out = torch.empty((300, n), dtype=torch.complex64, device="cuda")
+    for _ in range(3):
+        out.zero_()
+        p.execute(xd, out)
+    torch.cuda.synchronize()
+    p.close()
+    assert rel_l2(out.cpu().numpy(), oracle.cwt_fp64(x, sc, 2.0, 1, True)) < TOL
