@@ -39,6 +39,8 @@ cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
 cudaError_t launch_engine(const EngineParams& p, const CUtensorMap& omap, int grid, cudaStream_t st);
 cudaError_t tc_configure();
+cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const int* row_list, int n_list,
+                              const float* pool, float* wts, cudaStream_t st);
 cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st);
 }  // namespace fcwt
 
@@ -194,7 +196,7 @@ struct fcwt_plan {
     bool is_complex = false;
     std::vector<PlanSignal> sig;
     std::vector<PlanTables> tables;
-    DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs, tc_rows;
+    DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs, tc_rows, tc_wts;
     fcwt::FwdJob* jobs_host = nullptr;  // pinned staging of the batched forward jobs
     int n_items = 0;
     int n_rows = 0;
@@ -232,6 +234,7 @@ void plan_free(fcwt_plan* p) {
     p->fwd_tmp.release();
     p->graph_jobs.release();
     p->tc_rows.release();
+    p->tc_wts.release();
     if (p->jobs_host) cudaFreeHost(p->jobs_host);
     delete p;
 }
@@ -262,6 +265,7 @@ int plan_build(fcwt_plan* P) {
     std::vector<RowDesc> rows;
     std::vector<int> two_phase_rows;  // global indices, in order
     std::vector<int> tc_rows;         // rows of the tensor-core engine, in order
+    long long tc_wts_elems = 0;       // size of their weight table
     std::vector<Item> items;
     int max_two_phase_log2N = 0;
     for (int s = 0; s < nsig; s++) {
@@ -305,6 +309,11 @@ int plan_build(fcwt_plan* P) {
                 if (tc_kp) d.L = L;
             }
             d.kp = tc_kp;
+            d.woff = 0;
+            if (tc_kp) {
+                d.woff = tc_wts_elems;
+                tc_wts_elems += (long long)kP2 * tc_kp;
+            }
             rows.push_back(d);
             if (tc_kp) {
                 tc_rows.push_back(g);
@@ -396,6 +405,9 @@ int plan_build(fcwt_plan* P) {
         FCWT_CUDA_TRY(P->tc_rows.ensure(tc_rows.size() * sizeof(int)));
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->tc_rows.p, tc_rows.data(), tc_rows.size() * sizeof(int),
                                       cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(P->tc_wts.ensure((size_t)tc_wts_elems * sizeof(float)));
+        FCWT_CUDA_TRY(launch_tc_weights(P->sigs.as<SigDesc>(), P->rows.as<RowDesc>(), P->tc_rows.as<int>(),
+                                        (int)tc_rows.size(), P->pool.as<float>(), P->tc_wts.as<float>(), st));
     }
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;
@@ -528,6 +540,7 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         tp.row_list = P->tc_rows.as<int>();
         tp.n_list = P->n_tc;
         tp.stale_pool = ep.stale_pool;
+        tp.wts = P->tc_wts.as<float>();
         tp.counter = ctx->counters.as<unsigned>() + n_counters - 1;
         for (int s = 0; s < nsig; s++) tp.outs[s] = dout[s];
         tp.err = ep.err;

@@ -65,6 +65,7 @@ struct RowDesc {
     float ca, cb;     // continuous Morlet: u = ca*q - cb
     float cnorm;      // continuous Morlet amplitude (the mother table's norm)
     int kp;           // tensor-core rows: 1024-bin blocks of the window, padded to 8 or 16
+    long long woff;   // tensor-core rows: offset of the row's 1024*kp weights in the plan's table
 };
 
 enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3, ITEM_PHASE1W = 4 };
@@ -121,6 +122,7 @@ struct TcParams {
     const int* row_list;       // rows of this launch, in queue order
     int n_list;
     const float* stale_pool;
+    const float* wts;          // per-row daughter weights x out_scale on [L, L + 1024 kp)
     unsigned* counter;         // row queue head
     void* outs[kMaxOuts];
     int* err;

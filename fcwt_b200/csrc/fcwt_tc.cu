@@ -49,7 +49,8 @@ constexpr int kTcOffT2 = kTcOffTwlo + kP2 * 8;
 constexpr int kTcOffTwhi = kTcOffT2 + kP2 * 8;
 constexpr int kTcOffB = kTcOffTwhi + kTcTwhiSmem * 8;
 constexpr int kTcBBytes = 16 * 2 * kTcMaxKp * 2;  // one B operand (16 rows x 2Kp halves), 1 KB
-constexpr int kTcOffEnd = kTcOffB + 2 * 2 * kTcBBytes;
+constexpr int kTcOffTg = kTcOffB + 2 * 2 * kTcBBytes;
+constexpr int kTcOffEnd = kTcOffTg + 2 * 32 * 8;
 constexpr size_t kTcSmemBytes = (size_t)kTcOffEnd + 1024;
 static_assert(4 * kBoxBytes == kTcGbufBytes, "staging boxes fill one G buffer");
 
@@ -142,8 +143,9 @@ __device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, floa
 // K-major layout: (k / 16) * 512 + (n / 8) * 256 + ((k / 8) % 2) * 128 +
 // (n % 8) * 16 + (k % 8) * 2.
 template <int KP>
-__device__ __forceinline__ void build_b(int g, int ht, int M, unsigned Nm, int L, const float2* __restrict__ twlo,
+__device__ __forceinline__ void build_b(float2* __restrict__ tg, int g, int ht, int M, unsigned Nm, int L, const float2* __restrict__ twlo,
                                         const float2* __restrict__ twhi, unsigned char* bhi, unsigned char* blo) {
+    if (ht >= 224) tg[ht - 224] = tw_n(twlo, twhi, ((unsigned)(ht - 224) * (unsigned)(g * kTcCols)) & Nm);
     if (ht < kTcCols * KP) {
         const int j = ht / KP;
         const int k1 = ht - j * KP;
@@ -203,7 +205,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     // ---- pre-pass: Z on the window into tensor memory (split FP16)
     float scale, inv;
     {
-        const float nm1 = (float)N - 1.0f;
+        const float* __restrict__ wrow = P.wts + R.woff;
         const int tsel = warp >> 2;  // this warp's tiles: tsel, tsel + 4
         float2 z[2][KP];
         float mx = 0.0f;
@@ -212,7 +214,10 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             const int k2 = 128 * (tsel + 4 * ti) + 32 * qd + lane;
 #pragma unroll
             for (int k1 = 0; k1 < KP; k1++) {
-                const float2 v = bin_value(R, S, P.stale_pool, nm1, R.L + k2 + kP2 * k1);
+                const int q = R.L + k2 + kP2 * k1;
+                const float m = __ldg(wrow + k2 + kP2 * k1);
+                const float2 xv = (q >= R.lo && q < R.hi) ? __ldg(S.X + q) : make_float2(0.0f, 0.0f);
+                const float2 v = make_float2(xv.x * m, xv.y * m);
                 z[ti][k1] = v;
                 mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
             }
@@ -260,13 +265,14 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     float2* gbuf = reinterpret_cast<float2*>(sm + h * kTcGbufBytes);
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
     unsigned char* blo = bhi + kTcBBytes;
+    float2* tg = reinterpret_cast<float2*>(sm + kTcOffTg) + 32 * h;
     const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
     const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
     const bool tma = P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0;
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP>(g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
         fence_proxy_async_smem();
         half_bar(h);
         if (ht == 0) {
@@ -288,7 +294,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
             tmem_wait_ld();
             const int k2 = 128 * (tb + tt) + 32 * qd + lane;
-            float2 w = cscale(tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)c0) & Nm), inv);
+            float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], inv));
             const float2 stp = twlo[k2];
 #pragma unroll
             for (int j = 0; j < kTcCols; j++) {
@@ -300,7 +306,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (tma && ht == 0) bulk_wait_read_all();
         half_bar(h);  // accumulators drained; the G buffer is free
         const int gn = g + 2;
-        if (gn < ng) build_b<KP>(gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
             const int k2 = 128 * (tb + tt) + 32 * qd + lane;
@@ -432,7 +438,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
 }
 
+// Plan-time weight table of the tensor-core rows: wts[woff + i] = daughter
+// weight of bin q = L + i times out_scale (0 outside [lo, hi)), the same
+// float product the engines apply per bin, so that the per-row pre-pass reads
+// it with coalesced loads instead of gathering the mother table.
+__global__ void k_tc_weights(const SigDesc* __restrict__ sigs, const RowDesc* __restrict__ rows,
+                             const int* __restrict__ row_list, const float* __restrict__ pool,
+                             float* __restrict__ wts) {
+    const RowDesc R = rows[row_list[blockIdx.x]];
+    const SigDesc S = sigs[R.sig];
+    const float nm1 = (float)(1 << S.log2N) - 1.0f;
+    const int len = kP2 * R.kp;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const int q = R.L + i;
+        wts[R.woff + i] = (q >= R.lo && q < R.hi) ? bin_weight(R, S.mother, pool, nm1, q) * R.out_scale : 0.0f;
+    }
+}
+
 }  // namespace dev
+
+cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const int* row_list, int n_list,
+                              const float* pool, float* wts, cudaStream_t st) {
+    if (n_list <= 0) return cudaSuccess;
+    dev::k_tc_weights<<<n_list, 256, 0, st>>>(sigs, rows, row_list, pool, wts);
+    return cudaGetLastError();
+}
 
 size_t tc_smem_bytes() { return dev::kTcSmemBytes; }
 
