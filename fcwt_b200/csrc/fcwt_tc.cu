@@ -168,9 +168,8 @@ __device__ __forceinline__ void build_b(float2* __restrict__ tg, int g, int ht, 
 
 // The MMAs of one group: for each k2 tile, D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
 template <int KP>
-__device__ __forceinline__ void issue_group(uint32_t tmem, uint32_t dcol, uint32_t bhi, uint32_t blo) {
-#pragma unroll 1
-    for (int t = 0; t < 8; t++) {
+__device__ __forceinline__ void issue_group(int t, uint32_t tmem, uint32_t dcol, uint32_t bhi, uint32_t blo) {
+    {
         const uint32_t d = dcol + 16u * t;
 #pragma unroll
         for (int p = 0; p < 3; p++) {
@@ -275,9 +274,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
         fence_proxy_async_smem();
         half_bar(h);
-        if (ht == 0) {
+        if (lane == 0) {
             tc_fence_after();
-            issue_group<KP>(tmem, dcol, bhi_a, blo_a);
+            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
     }
@@ -303,7 +302,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             }
         }
         tc_fence_before();
-        if (tma && ht == 0) bulk_wait_read_all();
+        if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators drained; the G buffer is free
         const int gn = g + 2;
         if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
@@ -315,9 +314,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         }
         fence_proxy_async_smem();
         half_bar(h);  // G tiles and the next B in SMEM
-        if (ht == 0 && gn < ng) {
+        if (lane == 0 && gn < ng) {
             tc_fence_after();
-            issue_group<KP>(tmem, dcol, bhi_a, blo_a);
+            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
         // phase 2: one column per warp
@@ -336,9 +335,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             fence_proxy_async_smem();
             half_bar(h);
             const int n_full = n / M;
-            if (ht == 0) {
-                for (int j = 0; j < 4 && j * kBoxRows < n_full; j++)
-                    tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, R.out_row);
+            if (lane == 0 && wl >= 4) {
+                const int j = wl - 4;
+                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
             const int tail = n - n_full * M;
@@ -385,8 +384,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         t2[j] = make_float2((float)c, (float)s);
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[1])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_log2N = -1;
     }
@@ -431,7 +430,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
         tc_fence_after();
     }
-    if ((tid & 255) == 0 && P.tma_store) bulk_wait_all();
+    if ((tid & 31) == 0 && ((tid >> 5) & 7) >= 4 && P.tma_store) bulk_wait_all();
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
