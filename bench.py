@@ -40,6 +40,10 @@ N_SAMPLES = 100_000
 FS = 1000
 F0, F1, FN = 1.0, 101.0, 3000
 SIGMA = 2.0
+# DRAM bytes (read + write) of one k_row_tc launch of this workload: ncu
+# dram__bytes_read.sum 149.06 MB + dram__bytes_write.sum 2.35 GB (one-pass
+# capture of the full-size launch; profiles/k_row_tc_cwt100k_x3000.md)
+TRAFFIC_PER_LAUNCH = 149.06e6 + 2.35e9
 WORKLOAD = "cwt_100k_x_3000: real f32 n=100000 (N=131072) fs=1000, Morlet sigma=2, LINFREQS 1-101 Hz fn=3000, complex64 out"
 
 
@@ -195,6 +199,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fn", type=int, default=FN,
                     help="number of rows; values other than 3000 are for profiling captures only")
+    ap.add_argument("--no-forms", action="store_true", help="skip the BF16-output form of the default workload")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "grad", "long"],
+                    help="plain: the 100k x 3000 transform (default); batched: 384 uneven channels, one "
+                         "persistent launch vs a per-channel loop; grad: differentiable transform, forward + "
+                         "backward; long: complex 2^20 x 1024, BF16 vs complex64 output")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -204,6 +213,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload != "plain":
+        run_form(args)
         return
 
     import torch
@@ -294,6 +306,33 @@ def main():
                "ms_per_step": 1e3 * te / args.e2e_steps, "host_buffers": "pinned"}
         del xin, hout
 
+    # ---- BF16-output form of the same workload (half the output bytes)
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        outb = torch.empty((fn, N_SAMPLES, 2), dtype=torch.bfloat16, device=f"cuda:{dev}")
+        for _ in range(args.warmup):
+            plan.execute(xd, outb, out_type=fcwt.FCWT_OUT_BF16, stream=stream)
+        torch.cuda.synchronize(dev)
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(xd, outb, out_type=fcwt.FCWT_OUT_BF16, stream=stream)
+        b1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_b = b0.elapsed_time(b1) / args.steps
+        plan.execute(xd, out, stream=stream)
+        torch.cuda.synchronize(dev)
+        sel = torch.arange(0, fn, max(1, fn // 30), device=f"cuda:{dev}")
+        ref = out[sel].to(torch.complex128)
+        got = torch.complex(outb[sel, :, 0].double(), outb[sel, :, 1].double())
+        err = float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref))
+        forms = {"bf16_out": {"value": points / (ms_b / 1e3), "unit": "points/s", "ms_per_step": ms_b,
+                              "speedup_vs_complex64": ms_step / ms_b, "rel_l2_vs_complex64": err,
+                              "algorithmic_bytes": algorithmic_bytes(N_SAMPLES, fn, N, 4),
+                              "error_rows": int(sel.numel())}}
+        del outb
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.oracle import Reference
@@ -314,6 +353,12 @@ def main():
     if rank != 0:
         return
     peak, peak_kind = load_peaks()
+    st = plan.stats()
+    kname = ("k_row_tc" if st["tensor_core_rows"] == st["rows"] else
+             "k_row_engine" if st["tensor_core_rows"] == 0 else "k_row_tc + k_row_engine")
+    # DRAM bytes of one launch of the row kernel (read + write), from the ncu
+    # capture summarised in profiles/ (same workload); per launch like `achieved`
+    traffic = TRAFFIC_PER_LAUNCH if (fn == FN and kname == "k_row_tc") else None
     algo = algorithmic_bytes(N_SAMPLES, fn, N)
     achieved = algo / (eng_avg / 1e3) / 1e9
     line = {
@@ -325,12 +370,176 @@ def main():
                    "sigma": SIGMA, "scaling": "LINFREQS", "threads_param": 1, "out": "complex64",
                    "l2": "each step writes a 2.4 GB output (> 126 MB L2); no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "k_row_engine", "kernel_ms": eng_avg, "algorithmic_bytes": algo},
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": kname, "kernel_ms": eng_avg, "algorithmic_bytes": algo},
+        "forms": forms,
         "hbm_gbs_step": algo / (ms_step / 1e3) / 1e9,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": kernels,
     }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- other forms
+# Single-GPU workloads of the batched, differentiable and reduced-precision
+# forms. Each prints one JSON line of its own.
+
+def _timed(fn_step, steps: int, warmup: int, stream) -> float:
+    import torch
+
+    for _ in range(warmup):
+        fn_step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _pink_bursts(rng, n: int, fs: float) -> np.ndarray:
+    """Pink (1/f) noise shaped in the frequency domain plus bursts of 5-200 Hz
+    sinusoids at random onsets and durations; unit RMS."""
+    w = rng.standard_normal(n)
+    W = np.fft.rfft(w)
+    f = np.fft.rfftfreq(n, 1.0 / fs)
+    W[1:] /= np.sqrt(f[1:])
+    W[0] = 0
+    x = np.fft.irfft(W, n)
+    x /= np.std(x) + 1e-30
+    t = np.arange(n) / fs
+    for _ in range(int(rng.integers(2, 8))):
+        f0 = rng.uniform(5, 200)
+        a = int(rng.integers(0, n))
+        d = int(rng.integers(n // 50 + 1, n // 5 + 2))
+        x[a:a + d] += 2.0 * np.sin(2 * np.pi * f0 * t[a:a + d] + rng.uniform(0, 2 * np.pi))
+    return (x / np.sqrt(np.mean(x * x))).astype(np.float32)
+
+
+def run_form(args) -> None:
+    import torch
+
+    import fcwt_b200 as fcwt
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    steps, warmup = args.steps, max(args.warmup, 3)
+    sampler = ClockSampler(dev)
+    line = {"n_gpus": 1, "steps": steps, "warmup": warmup, "data": "synthetic", "scaling": "weak",
+            "vs_baseline": None}
+    if args.workload == "batched":
+        # 384 real channels, lengths U[20000, 200000] at 30 kHz, Morlet sigma 6, per-channel
+        # LOGSCALES grids of U[64, 256] frequencies in 1-5000 Hz, complex64 outputs
+        rng = np.random.default_rng(2024)
+        C = 384
+        ns = [int(v) for v in rng.integers(20000, 200001, C)]
+        fns = [int(v) for v in rng.integers(64, 257, C)]
+        morl = fcwt.Morlet(6.0)
+        grids = [fcwt.Scales(morl, fcwt.FCWT_LOGSCALES, 30000, 1.0, 5000.0, k).scales for k in fns]
+        xs = [torch.from_numpy(_pink_bursts(rng, n, 30000.0)).cuda() for n in ns]
+        outs = [torch.empty((k, n), dtype=torch.complex64, device="cuda") for k, n in zip(fns, ns)]
+        points = sum(k * n for k, n in zip(fns, ns))
+        plans = [fcwt.Plan(n, g, fb=6.0, threads=1, norm=True) for n, g in zip(ns, grids)]
+        bp = fcwt.BatchPlan(ns, grids, fb=6.0, threads=1, norm=True)
+
+        def loop():
+            for p, x, o in zip(plans, xs, outs):
+                p.execute(x, o, stream=stream)
+
+        def batched():
+            bp.execute(xs, outs, graph=True, stream=stream)
+
+        ms_loop = _timed(loop, steps, warmup, stream)
+        sampler.start()
+        ms_b = _timed(batched, steps, warmup, stream)
+        clocks = sampler.stop()
+        st = bp.stats()
+        line.update({"metric": "scalogram points/s", "value": points / (ms_b / 1e3), "unit": "points/s",
+                     "ms_per_step": ms_b, "higher_is_better": True, "dtype": "f32",
+                     "config": {"workload": "batched_384ch: real f32 channels n~U[20000,200000] fs=30000, "
+                                            "Morlet sigma=6, LOGSCALES 1-5000 Hz fn~U[64,256], complex64 out",
+                                "channels": C, "points": points, "output_bytes": 8 * points,
+                                "rows": st["rows"], "tensor_core_rows": st["tensor_core_rows"]},
+                     "plain_loop": {"value": points / (ms_loop / 1e3), "ms_per_step": ms_loop,
+                                    "what": "one plan per channel executed in a loop on one stream"},
+                     "speedup_vs_plain_loop": ms_loop / ms_b,
+                     "hbm_gbs": 8 * points / (ms_b / 1e3) / 1e9, "clocks": clocks})
+    elif args.workload == "grad":
+        # 64 x 16384 real signals at 1 kHz, learnable sigma (2.0) and 128 log-spaced centre
+        # frequencies 2-200 Hz; loss = MSE(|W|^2, seeded target); forward + backward
+        from fcwt_b200.autograd import LearnableMorletCWT
+
+        rng = np.random.default_rng(7)
+        B, n, F = 64, 16384, 128
+        t = np.arange(n) / 1000.0
+        env = np.exp(-0.5 * ((t - t.mean()) / (0.25 * t.max())) ** 2)
+        xs = np.stack([env * np.sin(2 * np.pi * (rng.uniform(2, 50) + rng.uniform(10, 100) * t) * t)
+                       + 0.1 * rng.standard_normal(n) for _ in range(B)]).astype(np.float32)
+        x = torch.from_numpy(xs).cuda().requires_grad_(True)
+        layer = LearnableMorletCWT(np.geomspace(2.0, 200.0, F), 1000.0, sigma=2.0)
+        target = torch.from_numpy(rng.uniform(0, 1e-3, (B, F, n)).astype(np.float32)).cuda()
+
+        def step():
+            x.grad = None
+            layer.zero_grad()
+            y = layer(x)
+            loss = ((y.real ** 2 + y.imag ** 2 - target) ** 2).mean()
+            loss.backward()
+
+        def fwd():
+            with torch.no_grad():
+                layer(x)
+
+        ms_f = _timed(fwd, steps, warmup, stream)
+        sampler.start()
+        ms = _timed(step, steps, warmup, stream)
+        clocks = sampler.stop()
+        points = B * F * n
+        line.update({"metric": "scalogram points/s (forward + backward)", "value": points / (ms / 1e3),
+                     "unit": "points/s", "ms_per_step": ms, "higher_is_better": True, "dtype": "f32",
+                     "config": {"workload": "grad_64x16384x128: batch 64 real f32 n=16384 fs=1000, learnable "
+                                            "sigma (2.0) and 128 centre frequencies 2-200 Hz, loss MSE(|W|^2, target)",
+                                "batch": B, "n": n, "fn": F},
+                     "forward_ms": ms_f, "clocks": clocks,
+                     "note": "step = forward transform + loss + hand-written adjoint (signal, sigma, frequencies)"})
+    else:
+        # complex 2^20 (independent AR(1) phi = 0.95 real and imaginary parts) at 200 kHz,
+        # Morlet sigma 4, 1024 LOGSCALES frequencies 10 Hz - 80 kHz; BF16 vs complex64 output
+        rng = np.random.default_rng(5)
+        n, F = 1 << 20, 1024
+        e = rng.standard_normal((2, n))
+        from scipy.signal import lfilter
+
+        ar = lfilter([1.0], [1.0, -0.95], e, axis=1)
+        x = (ar[0] + 1j * ar[1]).astype(np.complex64)
+        sc = fcwt.Scales(fcwt.Morlet(4.0), fcwt.FCWT_LOGSCALES, 200000, 10.0, 80000.0, F)
+        plan = fcwt.Plan(n, sc, fb=4.0, threads=1, norm=True, complex_input=True)
+        xd = torch.from_numpy(x).cuda()
+        out64 = torch.empty((F, n), dtype=torch.complex64, device="cuda")
+        ms64 = _timed(lambda: plan.execute(xd, out64, stream=stream), steps, warmup, stream)
+        out16 = torch.empty((F, n, 2), dtype=torch.bfloat16, device="cuda")
+        sampler.start()
+        ms16 = _timed(lambda: plan.execute(xd, out16, out_type=fcwt.FCWT_OUT_BF16, stream=stream), steps, warmup,
+                      stream)
+        clocks = sampler.stop()
+        sel = torch.arange(0, F, 16, device="cuda")
+        ref = out64[sel].to(torch.complex128)
+        got = torch.complex(out16[sel, :, 0].double(), out16[sel, :, 1].double())
+        err = float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref))
+        st = plan.stats()
+        points = n * F
+        line.update({"metric": "scalogram points/s (BF16 output)", "value": points / (ms16 / 1e3),
+                     "unit": "points/s", "ms_per_step": ms16, "higher_is_better": True, "dtype": "f32",
+                     "config": {"workload": "long_complex_2^20_x_1024: complex f32 AR(1) n=2^20 fs=200000, Morlet "
+                                            "sigma=4, LOGSCALES 10 Hz-80 kHz fn=1024, BF16 complex out",
+                                "rows": st["rows"], "tensor_core_rows": st["tensor_core_rows"]},
+                     "complex64_out": {"value": points / (ms64 / 1e3), "ms_per_step": ms64},
+                     "speedup_vs_complex64": ms64 / ms16, "rel_l2_bf16_vs_complex64": err,
+                     "hbm_gbs_bf16": 4 * points / (ms16 / 1e3) / 1e9, "clocks": clocks})
     print(json.dumps(line))
 
 

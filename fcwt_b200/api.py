@@ -335,6 +335,12 @@ class Plan:
         _check_host_output(out, self.n_rows, self.n, out_type)
         _lib.call("fcwt_plan_execute", self.handle, _ptr(xin), _ptr(out), out_type)
 
+    def stats(self) -> dict:
+        """Rows of the plan and how many run on the tensor-core engine."""
+        r, t = ctypes.c_int(), ctypes.c_int()
+        _lib.call("fcwt_plan_stats", self.handle, ctypes.byref(r), ctypes.byref(t))
+        return {"rows": r.value, "tensor_core_rows": t.value}
+
     def execute_ptr(self, x_ptr: int, out_ptr: int, out_type: int = FCWT_OUT_C64, stream_ptr: int | None = None) -> None:
         """Raw-pointer form (device or host pointers); stream_ptr None = the
         context's own stream, 0 = legacy default stream."""
@@ -384,6 +390,12 @@ class BatchPlan:
         _lib.call("fcwt_plan_create_batched", self.ctx.handle, nsig, ns_arr, 1 if complex_input else 0,
                   ctypes.c_float(fb), sc_arr, fns_arr, int(threads), flags, ctypes.byref(h))
         self.handle = h
+
+    def stats(self) -> dict:
+        """Rows of the plan and how many run on the tensor-core engine."""
+        r, t = ctypes.c_int(), ctypes.c_int()
+        _lib.call("fcwt_plan_stats", self.handle, ctypes.byref(r), ctypes.byref(t))
+        return {"rows": r.value, "tensor_core_rows": t.value}
 
     def outputs_like(self, device=None, out_dtype=None):
         """Allocate torch outputs [fn_s, n_s] (complex64) for every signal."""

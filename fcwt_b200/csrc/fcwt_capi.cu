@@ -413,6 +413,10 @@ int plan_build(fcwt_plan* P) {
     return FCWT_OK;
 }
 
+// Queue counters of one execution: [0] item queue; a_done[rows]; b_done[rows];
+// tensor-core row queue.
+size_t plan_counters(const fcwt_plan* P) { return 2 + 2 * (size_t)P->n_rows; }
+
 // (table, count) groups of the batched forward jobs, in table order.
 void job_groups(const fcwt_plan* P, std::vector<std::pair<int, int>>& groups) {
     groups.clear();
@@ -489,8 +493,7 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
             off += g.second;
         }
     }
-    // [0]: item queue; a_done[rows]; b_done[rows]; tensor-core row queue
-    const size_t n_counters = 2 + 2 * (size_t)P->n_rows;
+    const size_t n_counters = plan_counters(P);
     FCWT_CUDA_TRY(ctx->counters.ensure(n_counters * sizeof(unsigned)));
     FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, n_counters * sizeof(unsigned), st));
     FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
@@ -1000,7 +1003,7 @@ int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* co
         size_t maxN = 1;
         for (auto& S : plan->sig) maxN = std::max(maxN, (size_t)S.sp.N);
         FCWT_CUDA_TRY(ctx->tmp.ensure(maxN * sizeof(float2)));
-        FCWT_CUDA_TRY(ctx->counters.ensure((1 + 2 * (size_t)plan->n_rows) * sizeof(unsigned)));
+        FCWT_CUDA_TRY(ctx->counters.ensure(plan_counters(plan) * sizeof(unsigned)));
         FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
         if (plan->two_phase)
             FCWT_CUDA_TRY(ctx->scratch.ensure((size_t)plan->slots * (size_t)plan->slot_elems * sizeof(float2)));
@@ -1043,6 +1046,13 @@ int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* co
         plan->graph_out_type = out_type;
     }
     FCWT_CUDA_TRY(cudaGraphLaunch(plan->graph, st));
+    return FCWT_OK;
+}
+
+int fcwt_plan_stats(const fcwt_plan* plan, int* rows, int* tensor_core_rows) {
+    if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (rows) *rows = plan->n_rows;
+    if (tensor_core_rows) *tensor_core_rows = plan->n_tc;
     return FCWT_OK;
 }
 

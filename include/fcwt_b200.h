@@ -131,6 +131,9 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
                      int threads, unsigned flags, int row_begin, int row_end, fcwt_plan** plan);
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type);
 int fcwt_plan_destroy(fcwt_plan* plan);
+/* Introspection (no reference counterpart): rows the plan produces and how many
+ * of them the tensor-core engine runs (the rest run on the CUDA-core engine). */
+int fcwt_plan_stats(const fcwt_plan* plan, int* rows, int* tensor_core_rows);
 
 /* Batched plan: nsig signals (lengths ns[s], scale grids scales[s] of fns[s]
  * rows, one Morlet(fb)) transformed by one forward-FFT sequence per padded

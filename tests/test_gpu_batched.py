@@ -77,3 +77,25 @@ def test_graph_replay(fcwt, oracle):
         assert torch.allclose(a, -0.5 * b, rtol=1e-5, atol=1e-6)
     fcwt.synchronize()
     bp.close()
+
+
+def test_graph_first_execution_of_a_larger_plan(fcwt, oracle):
+    """A graph captured for a plan with more rows than any earlier execution
+    of the process: every per-execution buffer is sized before the capture
+    starts (nothing may allocate while the stream is capturing)."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    lengths = [3000, 2500, 4000, 3500]
+    grids = [oracle.scales(LOGSCALES, 30000, 1.0, 5000.0, 2500) for _ in lengths]
+    xs = [torch.from_numpy(rng.standard_normal(n).astype(np.float32)).cuda() for n in lengths]
+    bp = fcwt.BatchPlan(lengths, grids, fb=6.0, threads=1)
+    outs = bp.outputs_like()
+    bp.execute(xs, outs, graph=True)
+    torch.cuda.synchronize()
+    ref = bp.outputs_like()
+    bp.execute(xs, ref)
+    torch.cuda.synchronize()
+    for a, b in zip(outs, ref):
+        assert torch.equal(a, b)
+    bp.close()
