@@ -140,6 +140,22 @@ bool encode_output_map(void* base, int n, int M, int rows, CUtensorMap* map) {
     return r == CUDA_SUCCESS;
 }
 
+// Tensor map of a 16-bit complex output (one 4-byte element per sample),
+// boxes of [256 a][8 columns], 32-byte swizzle. n must be a multiple of 4 so
+// that the row stride is a multiple of 16 bytes.
+bool encode_output_map16(void* base, int n, int M, int rows, CUtensorMap* map) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (n & 3) || ((uintptr_t)base & 15) || n / M < 1 || rows < 1) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)M, (cuuint64_t)(n / M), (cuuint64_t)rows};
+    cuuint64_t strides[2] = {(cuuint64_t)M * 4, (cuuint64_t)n * 4};
+    cuuint32_t box[3] = {8, 256, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 struct fcwt_plan;
@@ -517,11 +533,15 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     CUtensorMap omap;
     std::memset(&omap, 0, sizeof(omap));
     int map_ok = 0;
-    if (nsig == 1 && out_type == FCWT_OUT_C64 && (P->two_phase || P->n_tc > 0)) {
+    if (nsig == 1 && (P->two_phase || P->n_tc > 0)) {
         const PlanSignal& S = P->sig[0];
-        map_ok = encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
+        if (out_type == FCWT_OUT_C64)
+            map_ok = encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
+        else
+            map_ok = encode_output_map16(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
     }
-    ep.tma_store = P->two_phase ? map_ok : 0;
+    // the CUDA-core engine stages complex64 boxes only
+    ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64) ? map_ok : 0;
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     const bool prof = ctx->profiling && allow_profiling;

@@ -91,6 +91,25 @@ __device__ __forceinline__ unsigned stage_off(int a, int w) {
     const unsigned lin = (unsigned)((a & (kBoxRows - 1)) * (kGroupCols * 8) + w * 8);
     return (unsigned)(a >> 8) * kBoxBytes + (lin ^ (((lin >> 7) & 3u) << 4));
 }
+// The same for 4-byte outputs (BF16 / FP16 complex pairs): boxes of
+// [256 a][8 columns] x 4 bytes in the 32B-swizzled layout (16-byte chunk bit 4
+// XOR address bit 7).
+__device__ __forceinline__ unsigned stage16_off(int a, int w) {
+    const unsigned lin = (unsigned)((a & (kBoxRows - 1)) * (kGroupCols * 4) + w * 4);
+    return (unsigned)(a >> 8) * (kBoxBytes / 2) + (lin ^ (((lin >> 7) & 1u) << 4));
+}
+
+// Complex value as the 4-byte pair of a 16-bit output type.
+template <int OT>
+__device__ __forceinline__ unsigned pack16(float2 v) {
+    if constexpr (OT == OUT_BF16) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+        return *reinterpret_cast<unsigned*>(&h);
+    } else {
+        __half2 h = __floats2half2_rn(v.x, v.y);
+        return *reinterpret_cast<unsigned*>(&h);
+    }
+}
 
 // w_N^e with e < N from the low table (SMEM) and the high table (SMEM when
 // M <= 1024, else global).

@@ -267,7 +267,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     float2* tg = reinterpret_cast<float2*>(sm + kTcOffTg) + 32 * h;
     const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
     const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
-    const bool tma = P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0;
+    const bool tma = P.tma_store != 0 && R.out_buf == 0;  // the map matches the output type
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
@@ -328,30 +328,48 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         dft1024_warp_xor(x, lane, col, t2);
         half_bar(h);  // every column is in registers
         unsigned char* stage = reinterpret_cast<unsigned char*>(gbuf);
+        if constexpr (OT == OUT_C64) {
 #pragma unroll
-        for (int hh = 0; hh < 32; hh++) *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * hh, wl)) = x[hh];
+            for (int hh = 0; hh < 32; hh++)
+                *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * hh, wl)) = x[hh];
+        } else {
+#pragma unroll
+            for (int hh = 0; hh < 32; hh++)
+                *reinterpret_cast<unsigned*>(stage + stage16_off(lane + 32 * hh, wl)) = pack16<OT>(x[hh]);
+        }
         const long long row0 = R.out_off + c0;
+        constexpr int box_bytes = OT == OUT_C64 ? kBoxBytes : kBoxBytes / 2;
         if (tma) {
             fence_proxy_async_smem();
             half_bar(h);
             const int n_full = n / M;
             if (lane == 0 && wl >= 4) {
                 const int j = wl - 4;
-                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, R.out_row);
+                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
             const int tail = n - n_full * M;
-            if (ht < kTcCols && c0 + ht < tail && n_full < kP2)
-                store_out<OT>(outb, row0 + ht + (long long)M * n_full,
-                              *reinterpret_cast<const float2*>(stage + stage_off(n_full, ht)));
+            if (ht < kTcCols && c0 + ht < tail && n_full < kP2) {
+                const long long idx = row0 + ht + (long long)M * n_full;
+                if constexpr (OT == OUT_C64)
+                    store_out<OT>(outb, idx, *reinterpret_cast<const float2*>(stage + stage_off(n_full, ht)));
+                else
+                    __stcs(reinterpret_cast<unsigned*>(outb) + idx,
+                           *reinterpret_cast<const unsigned*>(stage + stage16_off(n_full, ht)));
+            }
         } else {
             half_bar(h);
             for (int idx = ht; idx < kTcCols * kP2; idx += 256) {
                 const int w = idx & (kTcCols - 1);
                 const int a = idx >> 3;
-                if (c0 + w + (long long)M * a < n)
-                    store_out<OT>(outb, row0 + w + (long long)M * a,
-                                  *reinterpret_cast<const float2*>(stage + stage_off(a, w)));
+                if (c0 + w + (long long)M * a < n) {
+                    const long long o = row0 + w + (long long)M * a;
+                    if constexpr (OT == OUT_C64)
+                        store_out<OT>(outb, o, *reinterpret_cast<const float2*>(stage + stage_off(a, w)));
+                    else
+                        __stcs(reinterpret_cast<unsigned*>(outb) + o,
+                               *reinterpret_cast<const unsigned*>(stage + stage16_off(a, w)));
+                }
             }
         }
         g = gn;

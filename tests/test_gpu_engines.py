@@ -100,11 +100,13 @@ def test_tensor_engine_complex_input_odd_n(fcwt, oracle, ctx):
     assert rel_l2(tc, ref) < TOL
 
 
+@pytest.mark.parametrize("n", [100000, 40002], ids=["tensor_map_stores", "plain_stores"])
 @pytest.mark.parametrize("out_type", [1, 2], ids=["bf16", "f16"])
-def test_tensor_engine_16bit_outputs(fcwt, oracle, ctx, out_type):
+def test_tensor_engine_16bit_outputs(fcwt, oracle, ctx, out_type, n):
+    """16-bit outputs: tensor-map stores when n is a multiple of 4 (16-byte row
+    stride), plain stores otherwise."""
     from fcwt_b200 import _lib
 
-    n = 100000
     rng = np.random.default_rng(3)
     x = rng.standard_normal(n).astype(np.float32)
     sc = oracle.scales(LINFREQS, 1000, 1.0, 101.0, 32)
