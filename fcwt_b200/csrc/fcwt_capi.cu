@@ -93,6 +93,7 @@ struct DevBuf {
 struct TuneChoice {
     int scratch_mb = 64;  // budget of the scratch ring
     int lag = 12;         // rows between a row's phase 1 and phase 2 items
+    int engine = 0;       // 0: tensor-core engine for the rows it takes; 1: CUDA-core engine only
 };
 
 bool is_device_pointer(const void* p) {
@@ -318,7 +319,9 @@ int plan_build(fcwt_plan* P) {
             const int g = (int)rows.size();
             // tensor-core rows: window [L, L + 1024 kp), L a multiple of 1024, kp <= 16
             int tc_kp = 0;
-            if (ctx->engine_mode != FCWT_ENGINE_CUDA_CORES && sp.N >= kTcMinN) {
+            const bool tc_on = ctx->engine_mode == FCWT_ENGINE_TENSOR_CORES ||
+                               (ctx->engine_mode == FCWT_ENGINE_AUTO && ctx->tune[sp.log2N].engine == 0);
+            if (tc_on && sp.N >= kTcMinN) {
                 const int L = rp.hi > rp.lo ? (rp.lo / kP2) * kP2 : 0;
                 const int kw = rp.hi > rp.lo ? (rp.hi - L + kP2 - 1) / kP2 : 0;
                 if (kw <= kTcMaxKp) tc_kp = kw <= 8 ? 8 : 16;
@@ -1259,6 +1262,8 @@ int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const cha
         } else if (key == "lag" && v >= 1 && v <= 64) {
             tc.lag = (int)v;
             got |= 2;
+        } else if (key == "engine" && (v == 0 || v == 1)) {
+            tc.engine = (int)v;
         }
     }
     if (got != 3) return fail(FCWT_ERR_IO, "optimization plan '" + path + "' is malformed");
@@ -1291,8 +1296,10 @@ int fcwt_create_optimization_plan(fcwt_context* ctx, int maxsize, int threads, i
             const int mbs[] = {16, 32, 64, 96};
             const int lags[] = {4, 8, 12, 16};
             const int nm = level == 1 ? 2 : (level == 2 ? 3 : 4);
+            // CUDA-core engine: scratch budget x lag grid; tensor-core engine: one candidate
             for (int a = 0; a < nm; a++)
-                for (int b = 0; b < nm; b++) cands.push_back({mbs[a + (4 - nm)], lags[b]});
+                for (int b = 0; b < nm; b++) cands.push_back({mbs[a + (4 - nm)], lags[b], 1});
+            if (N >= fcwt::kTcMinN) cands.push_back(TuneChoice{});
             // synthetic workload: N samples, 256 log-spaced scales over the band
             const int fn = 256;
             std::vector<float> sc((size_t)fn), x((size_t)N);
@@ -1341,8 +1348,13 @@ int fcwt_create_optimization_plan(fcwt_context* ctx, int maxsize, int threads, i
         f << "threads " << threads << "\n";
         f << "scratch_mb " << best.scratch_mb << "\n";
         f << "lag " << best.lag << "\n";
+        f << "engine " << best.engine << "\n";
         if (!f) return fail(FCWT_ERR_IO, "cannot write '" + path + "'");
     }
+    // cached plans were built with the previous choices
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& e : ctx->cache) plan_free(e.plan);
+    ctx->cache.clear();
     return FCWT_OK;
 }
 

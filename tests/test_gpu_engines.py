@@ -152,3 +152,20 @@ def test_tensor_engine_device_tensors_repeat(fcwt, oracle, ctx):
     torch.cuda.synchronize()
     p.close()
     assert rel_l2(out.cpu().numpy(), oracle.cwt_fp64(x, sc, 2.0, 1, True)) < TOL
+
+
+def test_tuner_records_engine_choice(fcwt, oracle, ctx, tmp_path, monkeypatch):
+    """create_FFT_optimization_plan times both row engines for lengths the
+    tensor-core engine can take and writes its choice into the plan file;
+    transforms that load the file use it and stay within tolerance."""
+    monkeypatch.chdir(tmp_path)
+    f = fcwt.FCWT(fcwt.Morlet(2.0), 1, True, True)
+    f.create_FFT_optimization_plan(20000, "FFTW_MEASURE")
+    lines = dict(ln.split() for ln in open("n32768_t1.wis").read().splitlines()[1:])
+    assert lines["engine"] in ("0", "1") and int(lines["N"]) == 32768
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(20000).astype(np.float32)
+    sc = fcwt.Scales(fcwt.Morlet(2.0), fcwt.FCWT_LOGSCALES, 1000, 1.0, 400.0, 64)
+    out = np.zeros((64, 20000), np.complex64)
+    f.cwt(x, sc, out)
+    assert rel_l2(out, oracle.cwt_fp64(x, sc.scales, 2.0, 1, True)) < TOL
