@@ -332,6 +332,22 @@ def main():
                               "algorithmic_bytes": algorithmic_bytes(N_SAMPLES, fn, N, 4),
                               "error_rows": int(sel.numel())}}
         del outb
+        # fused |W|^2 epilogue (float32 scalogram)
+        outp = torch.empty((fn, N_SAMPLES), dtype=torch.float32, device=f"cuda:{dev}")
+        for _ in range(args.warmup):
+            plan.execute(xd, outp, out_type=fcwt.FCWT_OUT_POWER, stream=stream)
+        torch.cuda.synchronize(dev)
+        b0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(xd, outp, out_type=fcwt.FCWT_OUT_POWER, stream=stream)
+        b1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_p = b0.elapsed_time(b1) / args.steps
+        pref = out[sel].abs().double() ** 2
+        perr = float(torch.linalg.vector_norm(outp[sel].double() - pref) / torch.linalg.vector_norm(pref))
+        forms["power_out"] = {"value": points / (ms_p / 1e3), "unit": "points/s", "ms_per_step": ms_p,
+                              "speedup_vs_complex64": ms_step / ms_p, "rel_l2_vs_complex64_abs2": perr}
+        del outp
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

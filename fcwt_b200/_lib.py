@@ -28,6 +28,8 @@ FCWT_CONTINUOUS = 1 << 3
 FCWT_OUT_C64 = 0
 FCWT_OUT_BF16 = 1
 FCWT_OUT_F16 = 2
+FCWT_OUT_POWER = 3
+FCWT_OUT_DB = 4
 
 FCWT_ENGINE_AUTO = 0
 FCWT_ENGINE_CUDA_CORES = 1

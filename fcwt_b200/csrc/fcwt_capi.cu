@@ -593,7 +593,7 @@ int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs
     fcwt_context* ctx = P->ctx;
     int rc = ctx_prepare(ctx);
     if (rc) return rc;
-    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
+    if (out_type < FCWT_OUT_C64 || out_type > FCWT_OUT_DB)
         return fail(FCWT_ERR_INVALID, "unknown output type");
     if (P->n_rows == 0) return FCWT_OK;
     const int nsig = (int)P->sig.size();
@@ -1005,7 +1005,7 @@ int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* co
     fcwt_context* ctx = plan->ctx;
     int rc = ctx_prepare(ctx);
     if (rc) return rc;
-    if (out_type != FCWT_OUT_C64 && out_type != FCWT_OUT_BF16 && out_type != FCWT_OUT_F16)
+    if (out_type < FCWT_OUT_C64 || out_type > FCWT_OUT_DB)
         return fail(FCWT_ERR_INVALID, "unknown output type");
     if (!inputs || !outputs) return fail(FCWT_ERR_INVALID, "null input or output array");
     const int nsig = (int)plan->sig.size();

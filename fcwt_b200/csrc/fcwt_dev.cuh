@@ -66,9 +66,12 @@ __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
     } else if constexpr (OT == OUT_BF16) {
         __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         __stcs(reinterpret_cast<unsigned*>(base) + idx, *reinterpret_cast<unsigned*>(&h));
-    } else {
+    } else if constexpr (OT == OUT_F16) {
         __half2 h = __floats2half2_rn(v.x, v.y);
         __stcs(reinterpret_cast<unsigned*>(base) + idx, *reinterpret_cast<unsigned*>(&h));
+    } else {
+        const float p = v.x * v.x + v.y * v.y;
+        __stcs(reinterpret_cast<float*>(base) + idx, OT == OUT_POWER ? p : 10.0f * log10f(p));
     }
 }
 
@@ -99,15 +102,19 @@ __device__ __forceinline__ unsigned stage16_off(int a, int w) {
     return (unsigned)(a >> 8) * (kBoxBytes / 2) + (lin ^ (((lin >> 7) & 1u) << 4));
 }
 
-// Complex value as the 4-byte pair of a 16-bit output type.
+// Complex value as the 4-byte element of a 4-byte output type (16-bit pair,
+// power or dB).
 template <int OT>
 __device__ __forceinline__ unsigned pack16(float2 v) {
     if constexpr (OT == OUT_BF16) {
         __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
         return *reinterpret_cast<unsigned*>(&h);
-    } else {
+    } else if constexpr (OT == OUT_F16) {
         __half2 h = __floats2half2_rn(v.x, v.y);
         return *reinterpret_cast<unsigned*>(&h);
+    } else {
+        const float p = v.x * v.x + v.y * v.y;
+        return __float_as_uint(OT == OUT_POWER ? p : 10.0f * log10f(p));
     }
 }
 

@@ -81,7 +81,7 @@ struct Item {
     int pad;
 };
 
-enum OutType : int { OUT_C64 = 0, OUT_BF16 = 1, OUT_F16 = 2 };
+enum OutType : int { OUT_C64 = 0, OUT_BF16 = 1, OUT_F16 = 2, OUT_POWER = 3, OUT_DB = 4 };
 
 // One signal of a batched forward FFT: input (real or complex), its length,
 // the spectrum it produces and a ping-pong buffer of N complex values.

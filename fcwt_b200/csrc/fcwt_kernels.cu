@@ -706,7 +706,13 @@ cudaError_t engine_configure() {
     e = cudaFuncSetAttribute(dev::k_row_engine<OUT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)dev::kEngineSmemBytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(dev::k_row_engine<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(dev::k_row_engine<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kEngineSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(dev::k_row_engine<OUT_POWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kEngineSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(dev::k_row_engine<OUT_DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dev::kEngineSmemBytes);
 }
 
@@ -720,6 +726,8 @@ cudaError_t launch_engine(const EngineParams& p, const CUtensorMap& omap, int gr
     switch (p.out_type) {
         case OUT_BF16: dev::k_row_engine<OUT_BF16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
         case OUT_F16: dev::k_row_engine<OUT_F16><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
+        case OUT_POWER: dev::k_row_engine<OUT_POWER><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
+        case OUT_DB: dev::k_row_engine<OUT_DB><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
         default: dev::k_row_engine<OUT_C64><<<grid, kThreads, dev::kEngineSmemBytes, st>>>(p, omap); break;
     }
     return cudaGetLastError();

@@ -490,7 +490,13 @@ cudaError_t tc_configure() {
     e = cudaFuncSetAttribute(dev::k_row_tc<OUT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)dev::kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(dev::k_row_tc<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_POWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dev::kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(dev::k_row_tc<OUT_DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dev::kTcSmemBytes);
 }
 
@@ -498,6 +504,8 @@ cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, 
     switch (out_type) {
         case OUT_BF16: dev::k_row_tc<OUT_BF16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
         case OUT_F16: dev::k_row_tc<OUT_F16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_POWER: dev::k_row_tc<OUT_POWER><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_DB: dev::k_row_tc<OUT_DB><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
         default: dev::k_row_tc<OUT_C64><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
     }
     return cudaGetLastError();

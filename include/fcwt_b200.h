@@ -48,6 +48,11 @@ extern "C" {
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
 #define FCWT_OUT_BF16 1  /* interleaved bfloat16 (re, im), 4 bytes per coefficient */
 #define FCWT_OUT_F16 2   /* interleaved float16 (re, im), 4 bytes per coefficient  */
+/* Fused epilogues (no reference counterpart: the reference's callers take
+ * np.abs(output) afterwards, boilerplate.py:46): the scalogram written
+ * directly, one float32 per coefficient (half the bytes of complex64). */
+#define FCWT_OUT_POWER 3 /* |W|^2 = re^2 + im^2, float32                          */
+#define FCWT_OUT_DB 4    /* 10 log10(|W|^2), float32 (-inf where |W| = 0)         */
 
 typedef struct fcwt_context fcwt_context;
 typedef struct fcwt_plan fcwt_plan;

@@ -169,3 +169,27 @@ def test_tuner_records_engine_choice(fcwt, oracle, ctx, tmp_path, monkeypatch):
     out = np.zeros((64, 20000), np.complex64)
     f.cwt(x, sc, out)
     assert rel_l2(out, oracle.cwt_fp64(x, sc.scales, 2.0, 1, True)) < TOL
+
+
+@pytest.mark.parametrize("mode", ["tensor_cores", "cuda_cores"])
+@pytest.mark.parametrize("n", [100000, 30001], ids=["tensor_map_stores", "plain_stores"])
+def test_power_and_db_epilogues(fcwt, oracle, ctx, mode, n):
+    """FCWT_OUT_POWER (|W|^2) and FCWT_OUT_DB (10 log10 |W|^2) written by the
+    row kernels equal the squared magnitude of the float64 oracle."""
+    from fcwt_b200 import _lib
+
+    m = _lib.FCWT_ENGINE_TENSOR_CORES if mode == "tensor_cores" else _lib.FCWT_ENGINE_CUDA_CORES
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal(n) + np.sin(np.arange(n) * 0.02)).astype(np.float32)
+    sc = oracle.scales(LINFREQS, 1000, 1.0, 101.0, 24)
+    ref = np.abs(oracle.cwt_fp64(x, sc, 2.0, 1, True)) ** 2
+    ctx.set_engine(m)
+    p = fcwt.Plan(n, sc, fb=2.0, threads=1, norm=True)
+    pw = np.zeros((24, n), np.float32)
+    db = np.zeros((24, n), np.float32)
+    p.execute(x, pw, out_type=fcwt.FCWT_OUT_POWER)
+    p.execute(x, db, out_type=fcwt.FCWT_OUT_DB)
+    p.close()
+    assert np.linalg.norm(pw - ref) / np.linalg.norm(ref) < 2e-5
+    mask = ref > 1e-6 * ref.max()
+    assert np.max(np.abs(db[mask] - 10 * np.log10(ref[mask]))) < 1e-3
