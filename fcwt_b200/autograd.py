@@ -25,6 +25,32 @@ from . import _lib
 from .api import BatchPlan
 
 
+_PLAN_CACHE: "OrderedDict" = None
+_PLAN_CACHE_SIZE = 4
+
+
+def _plan_for(dev: int, n: int, B: int, sig: float, scales: np.ndarray, norm: bool) -> BatchPlan:
+    """Batched continuous-Morlet plan, reused while the shape, bandwidth and
+    frequency grid stay the same (evaluation loops, frozen parameters); a
+    training step that moves sigma or the frequencies builds a new one."""
+    global _PLAN_CACHE
+    from collections import OrderedDict
+
+    if _PLAN_CACHE is None:
+        _PLAN_CACHE = OrderedDict()
+    key = (dev, n, B, float(np.float32(sig)), scales.tobytes(), bool(norm))
+    plan = _PLAN_CACHE.get(key)
+    if plan is not None:
+        _PLAN_CACHE.move_to_end(key)
+        return plan
+    plan = BatchPlan([n] * B, [scales] * B, fb=sig, norm=norm, device=dev, continuous=True)
+    _PLAN_CACHE[key] = plan
+    while len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+        _, old = _PLAN_CACHE.popitem(last=False)
+        old.close()
+    return plan
+
+
 class MorletCWTFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, sigma, freqs, fs: float, norm: bool = True):
@@ -38,10 +64,9 @@ class MorletCWTFunction(torch.autograd.Function):
             raise ValueError("sigma and frequencies must be positive")
         scales = (float(fs) / f).astype(np.float32)
         dev = x.device.index or 0
-        plan = BatchPlan([n] * B, [scales] * B, fb=sig, norm=norm, device=dev, continuous=True)
+        plan = _plan_for(dev, n, B, sig, scales, norm)
         y = torch.empty((B, f.size, n), dtype=torch.complex64, device=x.device)
         plan.execute([x[b] for b in range(B)], [y[b] for b in range(B)])
-        plan.close()
         ctx.save_for_backward(x)
         ctx.sig, ctx.f, ctx.fs, ctx.norm = sig, f, float(fs), bool(norm)
         ctx.sigma_like, ctx.freqs_like = sigma, freqs

@@ -12,6 +12,8 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <array>
+#include <map>
 #include <vector>
 
 #include "../../include/fcwt_b200.h"
@@ -283,6 +285,8 @@ int plan_build(fcwt_plan* P) {
     std::vector<int> two_phase_rows;  // global indices, in order
     std::vector<int> tc_rows;         // rows of the tensor-core engine, in order
     long long tc_wts_elems = 0;       // size of their weight table
+    std::vector<int> wts_rows;        // rows that own a weight-table entry
+    std::map<std::array<uint32_t, 12>, long long> wts_owner;
     std::vector<Item> items;
     int max_two_phase_log2N = 0;
     for (int s = 0; s < nsig; s++) {
@@ -330,8 +334,27 @@ int plan_build(fcwt_plan* P) {
             d.kp = tc_kp;
             d.woff = 0;
             if (tc_kp) {
-                d.woff = tc_wts_elems;
-                tc_wts_elems += (long long)kP2 * tc_kp;
+                // rows whose weights are the same function of q share one table entry
+                // (e.g. many channels on one grid); rows with stale bins never do
+                bool shared = false;
+                std::array<uint32_t, 12> key{};
+                if (d.stale < 0) {
+                    const float fk[6] = {d.step, d.ca, d.cb, d.cnorm, d.out_scale, 0.0f};
+                    key = {(uint32_t)sp.log2N, (uint32_t)d.mode, (uint32_t)d.L, (uint32_t)d.lo, (uint32_t)d.hi,
+                           (uint32_t)d.proc, (uint32_t)d.kp, 0, 0, 0, 0, 0};
+                    for (int k = 0; k < 5; k++) std::memcpy(&key[7 + k], &fk[k], 4);
+                    auto it = wts_owner.find(key);
+                    if (it != wts_owner.end()) {
+                        d.woff = it->second;
+                        shared = true;
+                    }
+                }
+                if (!shared) {
+                    d.woff = tc_wts_elems;
+                    tc_wts_elems += (long long)kP2 * tc_kp;
+                    if (d.stale < 0) wts_owner.emplace(key, d.woff);
+                    wts_rows.push_back((int)rows.size());
+                }
             }
             rows.push_back(d);
             if (tc_kp) {
@@ -425,8 +448,14 @@ int plan_build(fcwt_plan* P) {
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->tc_rows.p, tc_rows.data(), tc_rows.size() * sizeof(int),
                                       cudaMemcpyHostToDevice, st));
         FCWT_CUDA_TRY(P->tc_wts.ensure((size_t)tc_wts_elems * sizeof(float)));
-        FCWT_CUDA_TRY(launch_tc_weights(P->sigs.as<SigDesc>(), P->rows.as<RowDesc>(), P->tc_rows.as<int>(),
-                                        (int)tc_rows.size(), P->pool.as<float>(), P->tc_wts.as<float>(), st));
+        DevBuf owners;
+        FCWT_CUDA_TRY(owners.ensure(wts_rows.size() * sizeof(int)));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(owners.p, wts_rows.data(), wts_rows.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(launch_tc_weights(P->sigs.as<SigDesc>(), P->rows.as<RowDesc>(), owners.as<int>(),
+                                        (int)wts_rows.size(), P->pool.as<float>(), P->tc_wts.as<float>(), st));
+        FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+        owners.release();
     }
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;

@@ -281,6 +281,10 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         }
     }
     const int tb = (wl >> 2) * 4;  // this warp drains tiles tb .. tb + 3
+    const int amax = (n + M - 1) / M;  // stripes a that hold output samples
+    // the halves run the same per-group sequence; starting half 1 a little later
+    // keeps their DFT (issue-bound) and staging/store (SMEM-bound) phases apart
+    if (h == 1) __nanosleep(500);
     while (g < ng) {
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
@@ -331,11 +335,12 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if constexpr (OT == OUT_C64) {
 #pragma unroll
             for (int hh = 0; hh < 32; hh++)
-                *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * hh, wl)) = x[hh];
+                if (lane + 32 * hh < amax) *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * hh, wl)) = x[hh];
         } else {
 #pragma unroll
             for (int hh = 0; hh < 32; hh++)
-                *reinterpret_cast<unsigned*>(stage + stage16_off(lane + 32 * hh, wl)) = pack16<OT>(x[hh]);
+                if (lane + 32 * hh < amax)
+                    *reinterpret_cast<unsigned*>(stage + stage16_off(lane + 32 * hh, wl)) = pack16<OT>(x[hh]);
         }
         const long long row0 = R.out_off + c0;
         constexpr int box_bytes = OT == OUT_C64 ? kBoxBytes : kBoxBytes / 2;
