@@ -17,6 +17,10 @@ __all__ = ["Morlet", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCA
 
 
 def __getattr__(name):
+    if name == "StreamingCWT":
+        from .streaming import StreamingCWT
+
+        return StreamingCWT
     # the differentiable operator needs torch; import it on first use
     if name in ("morlet_cwt", "LearnableMorletCWT", "MorletCWTFunction"):
         from . import autograd
