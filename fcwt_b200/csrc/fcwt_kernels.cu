@@ -322,13 +322,100 @@ __device__ void phase1_wide(const SigDesc& S, const RowDesc& R, const float* __r
     }
 }
 
+// Phase 1 of a wide row with 64 <= K = 32 K2 <= 512, for k2 in [k2_0, k2_0 + 8).
+// The K-point DFT over k1 = j + K2 i is split as
+//     DFT_K[u1 + 32 u2] = sum_j w_K2^{j u2} w_K^{j u1} sum_i x[j + K2 i] w_32^{i u1}:
+// step B runs one register FFT32 over i per (v, j, k2) task, step C one
+// K2-point DFT over j per (v, u1, k2) task; every thread works in both steps.
+// The spectrum x weights of the 8 k2 columns are loaded into SMEM once per
+// item (zt[k1][8]); the FFT32 outputs of a batch of v values go through SMEM
+// (Y[u1][task], padded rows). Outputs: G[c = v + R u][k2] w_N^{(k2+L) c}.
+template <int K2>
+__device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
+                           const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                           float2* __restrict__ region0, float2* __restrict__ G) {
+    constexpr int K = 32 * K2;
+    constexpr int W = kWideChunk;
+    static_assert(W == 8, "task indexing assumes 8 k2 per item");
+    constexpr int kYPad = 4;
+    constexpr int VBmax = (kRegion0 - 32 * kYPad - K * W) / (K * W);
+    static_assert(VBmax >= 1, "zt and one batch of Y fit in region0");
+    const int tid = threadIdx.x;
+    const int log2N = S.log2N;
+    const int N = 1 << log2N;
+    const unsigned Nm = (unsigned)N - 1u;
+    const int M = N >> kLog2P2;
+    const unsigned Mm = (unsigned)M - 1u;
+    const int Rr = M / K;
+    const float nm1 = (float)N - 1.0f;
+    float2* zt = region0;
+    float2* Y = region0 + K * W;
+    for (int idx = tid; idx < K * W; idx += kThreads) {
+        const int k1 = idx >> 3;
+        const int kk = idx & 7;
+        zt[idx] = bin_value(R, S, pool, nm1, R.L + k2_0 + kk + kP2 * k1);
+    }
+    __syncthreads();
+    for (int v0 = 0; v0 < Rr; v0 += VBmax) {
+        const int VB = min(VBmax, Rr - v0);
+        const int T = VB * K2 * W;
+        const int TP = T + kYPad;
+        // (B) FFT32 over i, task t = (vb K2 + j) 8 + kk
+        for (int t = tid; t < T; t += kThreads) {
+            const int kk = t & 7;
+            const int j = (t >> 3) % K2;
+            const int v = v0 + (t >> 3) / K2;
+            // pre-twiddle w_M^{v k1}: exact table value every 8 steps, running product in between
+            const float2 stp = twhi[((unsigned)v * (unsigned)K2) & Mm];
+            float2 w = make_float2(1.0f, 0.0f);
+            float2 x[32];
+#pragma unroll
+            for (int i = 0; i < 32; i++) {
+                if ((i & 7) == 0) w = twhi[((unsigned)v * (unsigned)(j + K2 * i)) & Mm];
+                x[i] = cmul(zt[(j + K2 * i) * W + kk], w);
+                w = cmul(w, stp);
+            }
+            fft_reg<32, +1>(x);
+            // twiddle w_K^{j u1} = w_M^{j u1 R}
+            Y[t] = x[0];
+#pragma unroll
+            for (int u1 = 1; u1 < 32; u1++) Y[u1 * TP + t] = cmul(x[u1], twhi[((unsigned)(j * u1 * Rr)) & Mm]);
+        }
+        __syncthreads();
+        // (C) K2-point DFT over j, task t = (vb 32 + u1) 8 + kk
+        for (int t = tid; t < VB * 32 * W; t += kThreads) {
+            const int kk = t & 7;
+            const int u1 = (t >> 3) & 31;
+            const int vb = t >> 8;
+            float2 z[K2];
+#pragma unroll
+            for (int j = 0; j < K2; j++) z[j] = Y[u1 * TP + (vb * K2 + j) * W + kk];
+            fft_reg<K2, +1>(z);
+            const int k2 = k2_0 + kk;
+            const unsigned k2L = (unsigned)(k2 + R.L);
+            const unsigned c0 = (unsigned)(v0 + vb + Rr * u1);
+            const unsigned dc = (unsigned)(32 * Rr);
+            const float2 st = tw_n(twlo, twhi, (k2L * dc) & Nm);
+            float2 w = make_float2(1.0f, 0.0f);
+#pragma unroll
+            for (int u2 = 0; u2 < K2; u2++) {
+                const unsigned c = c0 + dc * (unsigned)u2;
+                if ((u2 & 7) == 0) w = tw_n(twlo, twhi, (k2L * c) & Nm);
+                __stcg(G + (size_t)c * kP2 + k2, cmul(z[u2], w));
+                w = cmul(w, st);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __device__ void phase1_wide_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool, int k2_0,
                                      const float2* twlo, const float2* twhi, float2* region0, float2* G) {
     switch (K) {
-        case 64: phase1_wide<2>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
-        case 128: phase1_wide<4>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
-        case 256: phase1_wide<8>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
-        case 512: phase1_wide<16>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 64: phase1_big<2>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 128: phase1_big<4>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 256: phase1_big<8>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
+        case 512: phase1_big<16>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
         default: phase1_wide<32>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
     }
 }
