@@ -65,6 +65,8 @@ SIGNATURES = {
     "fcwt_plan_execute": (_i, [_vp, _vp, _vp, _i]),
     "fcwt_plan_destroy": (_i, [_vp]),
     "fcwt_plan_stats": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "fcwt_plan_create_mother": (_i, [_vp, _i, _i, _vp, _i, _vp, _i, _i, _u, _i, _i, ctypes.POINTER(_vp)]),
+    "fcwt_cwt_mother": (_i, [_vp, _vp, _i, _i, _vp, _i, _vp, _i, _i, _u, _vp, _i]),
     "fcwt_plan_create_batched": (_i, [_vp, _i, _vp, _i, _f, _vp, _vp, _i, _u, ctypes.POINTER(_vp)]),
     "fcwt_plan_execute_batched": (_i, [_vp, _vp, _vp, _i]),
     "fcwt_plan_execute_graph": (_i, [_vp, _vp, _vp, _i]),

@@ -117,6 +117,43 @@ class Morlet(Wavelet):
         _lib.call("fcwt_morlet_wavelet", ctypes.c_float(self.fb), ctypes.c_float(scale), _ptr(pwav), pwav.size)
 
 
+
+class Paul(Wavelet):
+    """Paul wavelet of order m (analytic, single-sided, real in frequency).
+
+    The reference defines only Morlet; its test suite names Paul
+    (tests/test_fcwt.py:185-211, commented out). In the reference's
+    frequency variable x = 2 w (2 pi / N) of table entry w (Morlet's is
+    t = fb (x - 2 pi), src/fcwt/fcwt.cpp:51-67) this table is
+
+        mother[w] = A * y^m * exp(m (1 - y)),   y = x / (2 pi) = 2 w / N,
+
+    a Paul spectrum x^m e^{-x} stretched so its peak sits at x = 2 pi like the
+    Morlet's, so that Scales maps scale s to frequency fs / s for it too; A is
+    the Morlet table's peak value. The transform runs through the
+    caller-supplied-wavelet path (fcwt_cwt_mother)."""
+
+    def __init__(self, order: int = 4):
+        super().__init__()
+        self.m = int(order)
+        if self.m < 1:
+            raise ValueError("order must be >= 1")
+        self.four_wavelen = 1.0
+
+    def generate(self, *args):
+        if len(args) != 1:
+            raise NotImplementedError("Paul provides the frequency-domain table generate(size) only")
+        size = _as_int("size", args[0])
+        w = np.arange(max(size, 0), dtype=np.float64)
+        y = 2.0 * w / max(size, 1)
+        amp = np.sqrt(2.0 * np.pi) * 0.75112554446
+        with np.errstate(under="ignore"):
+            t = amp * np.exp(self.m * np.log(np.maximum(y, 1e-300)) + self.m * (1.0 - y))
+        t[y == 0] = 0.0
+        self.width = size
+        self.mother = t.astype(np.float32)
+        return None
+
 class Scales:
     """Scales(wavelet, scaletype, fs, f0, f1, fn) (src/fcwt/fcwt.cpp:111-190)."""
 
@@ -209,10 +246,34 @@ class FCWT:
         """FCWT::cwt(complex input, ...) (fcwt.cpp:545-548)."""
         self._run(pcinput, scales, poutput, True, out_type)
 
+    def _run_table(self, x, sc, out, complex_input: bool, out_type: int) -> None:
+        """Any other Wavelet subclass: the transform runs on its mother table."""
+        ctx = _lib.context(self.device)
+        if _is_torch(x) or _is_torch(out):
+            import torch
+
+            n = x.numel()
+            table = _table_of(self.wavelet, n)
+            ctx.set_stream(torch.cuda.current_stream(out.device).cuda_stream)
+            try:
+                _lib.call("fcwt_cwt_mother", ctx.handle, ctypes.c_void_p(x.data_ptr()), n, 1 if complex_input else 0,
+                          _ptr(table), table.size, _ptr(sc), sc.size, self.threads, self.flags,
+                          ctypes.c_void_p(out.data_ptr()), out_type)
+            finally:
+                ctx.set_stream(None)
+            return
+        xin = _host_input(x, complex_input)
+        n = xin.size
+        table = _table_of(self.wavelet, n)
+        _check_host_output(out, sc.size, n, out_type)
+        _lib.call("fcwt_cwt_mother", ctx.handle, _ptr(xin), n, 1 if complex_input else 0, _ptr(table), table.size,
+                  _ptr(sc), sc.size, self.threads, self.flags, _ptr(out), out_type)
+
     def _run(self, x, scales, out, complex_input: bool, out_type: int) -> None:
         sc = _scales_array(scales)
         if not isinstance(self.wavelet, Morlet):
-            raise TypeError("only the Morlet wavelet has a GPU transform")
+            self._run_table(x, sc, out, complex_input, out_type)
+            return
         fb = self.wavelet.fb
         ctx = _lib.context(self.device)
         fname = "fcwt_ccwt" if complex_input else "fcwt_cwt"
@@ -225,6 +286,19 @@ class FCWT:
         _check_host_output(out, sc.size, n, out_type)
         _lib.call(fname, ctx.handle, _ptr(xin), n, ctypes.c_float(fb), _ptr(sc), sc.size, self.threads,
                   self.flags, _ptr(out), out_type)
+
+
+def _table_of(wavelet, n: int) -> np.ndarray:
+    """The frequency-domain table wavelet.generate(N) fills, N = 2^find2power(n)
+    (the reference reads wavelet->mother after generate, fcwt.cpp:504-505)."""
+    if getattr(wavelet, "imag_frequency", False) or getattr(wavelet, "doublesided", False):
+        raise NotImplementedError("wavelets with imag_frequency or doublesided are not supported")
+    N = 1 << _lib.load().fcwt_find2power(int(n))
+    wavelet.generate(N)
+    t = getattr(wavelet, "mother", None)
+    if t is None or np.asarray(t).size != N:
+        raise ValueError(f"generate({N}) must leave a {N}-entry table in .mother")
+    return np.ascontiguousarray(t, np.float32)
 
 
 def _host_input(x, complex_input: bool) -> np.ndarray:

@@ -220,6 +220,7 @@ struct fcwt_plan {
     int n_items = 0;
     int n_rows = 0;
     int n_tc = 0;  // rows run by the tensor-core engine
+    std::vector<float> custom_mother;  // caller's wavelet table (N floats), empty for Morlet(fb)
     int slots = 0;
     long long slot_elems = 0;
     bool two_phase = false;
@@ -412,7 +413,11 @@ int plan_build(fcwt_plan* P) {
         const int M = N >= kP2 ? N / kP2 : 1;
         FCWT_CUDA_TRY(T.mother.ensure((size_t)N * sizeof(float)));
         FCWT_CUDA_TRY(T.tw.ensure((size_t)(1024 + M) * sizeof(float2)));
-        FCWT_CUDA_TRY(launch_mother(P->fb, N, host::mother_norm(), T.mother.as<float>(), st));
+        if (!P->custom_mother.empty() && (int)P->custom_mother.size() == N)
+            FCWT_CUDA_TRY(cudaMemcpyAsync(T.mother.p, P->custom_mother.data(), (size_t)N * sizeof(float),
+                                          cudaMemcpyHostToDevice, st));
+        else
+            FCWT_CUDA_TRY(launch_mother(P->fb, N, host::mother_norm(), T.mother.as<float>(), st));
         FCWT_CUDA_TRY(launch_twiddle(T.log2N, T.tw.as<float2>(), st));
     }
     std::vector<SigDesc> sds((size_t)nsig);
@@ -977,6 +982,63 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
     }
     *out = P;
     return FCWT_OK;
+}
+
+int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const float* mother, int mother_size,
+                            const float* scales, int fn, int threads, unsigned flags, int row_begin, int row_end,
+                            fcwt_plan** out) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (!out) return fail(FCWT_ERR_INVALID, "null plan output");
+    *out = nullptr;
+    if (fn < 0 || n < 0) return fail(FCWT_ERR_INVALID, "negative size");
+    if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
+    if (row_begin < 0 || row_end > fn || row_begin > row_end)
+        return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
+    if (flags & FCWT_CONTINUOUS) return fail(FCWT_ERR_INVALID, "FCWT_CONTINUOUS is the Morlet's own mode");
+    const int log2N = fcwt::host::find2power(n);
+    if (log2N > fcwt::kMaxLog2N) return fail(FCWT_ERR_INVALID, "signal too long: padded length exceeds 2^23");
+    const int N = 1 << log2N;
+    if (!mother || mother_size != N)
+        return fail(FCWT_ERR_INVALID, "the mother table must hold N = 2^find2power(n) = " + std::to_string(N) +
+                                          " values");
+    for (int i = 0; i < N; i++)
+        if (!std::isfinite(mother[i])) return fail(FCWT_ERR_INVALID, "the mother table holds a non-finite value");
+    fcwt_plan* P = new fcwt_plan();
+    P->ctx = ctx;
+    P->fb = 1.0f;
+    P->is_complex = is_complex != 0;
+    P->custom_mother.assign(mother, mother + N);
+    P->sig.resize(1);
+    P->sig[0].rb = row_begin;
+    P->sig[0].re = row_end;
+    std::string err;
+    if (fcwt::plan_signal(n, is_complex != 0, 1.0f, scales, fn, threads, flags, P->sig[0].sp, err, mother)) {
+        delete P;
+        return fail(FCWT_ERR_INVALID, err);
+    }
+    rc = plan_build(P);
+    if (rc) {
+        std::string keep = g_err;
+        plan_free(P);
+        g_err = keep;
+        return rc;
+    }
+    *out = P;
+    return FCWT_OK;
+}
+
+int fcwt_cwt_mother(fcwt_context* ctx, const void* input, int n, int is_complex, const float* mother,
+                    int mother_size, const float* scales, int fn, int threads, unsigned flags, void* output,
+                    int out_type) {
+    fcwt_plan* P = nullptr;
+    int rc = fcwt_plan_create_mother(ctx, n, is_complex, mother, mother_size, scales, fn, threads, flags, 0, fn, &P);
+    if (rc) return rc;
+    rc = plan_run(P, input, output, out_type);
+    std::string keep = g_err;
+    fcwt_plan_destroy(P);
+    g_err = keep;
+    return rc;
 }
 
 int fcwt_plan_create_batched(fcwt_context* ctx, int nsig, const int* ns, int is_complex, float fb,

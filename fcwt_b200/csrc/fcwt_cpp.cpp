@@ -138,7 +138,7 @@ void FCWT::create_FFT_optimization_plan(int pmaxsize, std::string flags) {
 
 void FCWT::run(const void* input, bool complexinput, int psize, std::complex<float>* poutput, Scales* scales) {
     Morlet* m = dynamic_cast<Morlet*>(wavelet);
-    if (!m) throw std::runtime_error("fcwt: only the Morlet wavelet has a GPU transform");
+    if (!wavelet) throw std::runtime_error("fcwt: null Wavelet");
     if (!scales) throw std::runtime_error("fcwt: null Scales");
     fcwt_context* ctx = t_ctx.get();
     if (use_optimalization_schemes) {
@@ -152,6 +152,19 @@ void FCWT::run(const void* input, bool complexinput, int psize, std::complex<flo
     }
     const unsigned flags = use_normalization ? FCWT_NORM : 0u;
     const float* in = reinterpret_cast<const float*>(input);
+    if (!m) {
+        // any other Wavelet: the table its generate(N) fills, as the reference uses it
+        // (src/fcwt/fcwt.cpp:504-505); single-sided real wavelets only
+        if (wavelet->imag_frequency || wavelet->doublesided)
+            throw std::runtime_error("fcwt: wavelets with imag_frequency or doublesided are not supported");
+        const int N = 1 << find2power(psize);
+        wavelet->generate(N);
+        if (!wavelet->mother) throw std::runtime_error("fcwt: Wavelet::generate(N) left mother empty");
+        check(fcwt_cwt_mother(ctx, input, psize, complexinput ? 1 : 0, wavelet->mother, N, scales->scales,
+                              scales->nscales, threads, flags, poutput, FCWT_OUT_C64));
+        check(fcwt_synchronize(ctx));
+        return;
+    }
     int rc = complexinput
                  ? fcwt_ccwt(ctx, in, psize, m->fb, scales->scales, scales->nscales, threads, flags, poutput, FCWT_OUT_C64)
                  : fcwt_cwt(ctx, in, psize, m->fb, scales->scales, scales->nscales, threads, flags, poutput, FCWT_OUT_C64);

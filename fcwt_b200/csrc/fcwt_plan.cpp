@@ -50,7 +50,7 @@ int first_true(int a, int b, F pred) {
 }  // namespace
 
 int plan_signal(int n, bool is_complex, float fb, const float* scales, int fn, int threads,
-                unsigned flags, SignalPlan& out, std::string& err) {
+                unsigned flags, SignalPlan& out, std::string& err, const float* mother_in) {
     if (n < 0) {
         err = "signal length must be >= 0";
         return 1;
@@ -179,13 +179,16 @@ int plan_signal(int n, bool is_complex, float fb, const float* scales, int fn, i
     // ---- significant mother indices (for trimming negligible weights).
     if (!exact) {
         std::vector<float> mother((size_t)N);
-        host::mother_table(fb, N, mother.data());
+        if (mother_in)
+            std::copy(mother_in, mother_in + N, mother.begin());
+        else
+            host::mother_table(fb, N, mother.data());
         float mx = 0.0f;
-        for (float v : mother) mx = std::max(mx, v);
+        for (float v : mother) mx = std::max(mx, std::fabs(v));
         const double thr = kTrimRel * (double)mx;
         int wl = 0, wh = N - 1;
-        while (wl < N && (double)mother[(size_t)wl] < thr) wl++;
-        while (wh >= 0 && (double)mother[(size_t)wh] < thr) wh--;
+        while (wl < N && std::fabs((double)mother[(size_t)wl]) < thr) wl++;
+        while (wh >= 0 && std::fabs((double)mother[(size_t)wh]) < thr) wh--;
         out.w_lo = wl;
         out.w_hi = wh;
     } else {

@@ -42,8 +42,9 @@ struct SignalPlan {
     int w_lo = 0, w_hi = -1;                // mother indices with non-negligible weight
 };
 
-// Returns 0 on success, otherwise fills `err`.
+// Returns 0 on success, otherwise fills `err`. `mother` (N floats) replaces the
+// Morlet(fb) table for trimming when the caller supplies its own wavelet.
 int plan_signal(int n, bool is_complex, float fb, const float* scales, int fn, int threads,
-                unsigned flags, SignalPlan& out, std::string& err);
+                unsigned flags, SignalPlan& out, std::string& err, const float* mother = nullptr);
 
 }  // namespace fcwt

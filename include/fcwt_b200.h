@@ -136,6 +136,18 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
                      int threads, unsigned flags, int row_begin, int row_end, fcwt_plan** plan);
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type);
 int fcwt_plan_destroy(fcwt_plan* plan);
+/* A caller-supplied wavelet: the reference's FCWT::cwt takes any Wavelet*
+ * and uses the table its generate(N) fills (src/fcwt/fcwt.cpp:504-505,
+ * fcwt.h:67-79). `mother` (host memory) holds that table, N =
+ * 2^find2power(n) floats; single-sided real wavelets (imag_frequency and
+ * doublesided false, the only kind the reference defines). Truncation,
+ * indices and reused bins follow the reference exactly as for Morlet. */
+int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const float* mother, int mother_size,
+                            const float* scales, int fn, int threads, unsigned flags, int row_begin, int row_end,
+                            fcwt_plan** plan);
+int fcwt_cwt_mother(fcwt_context* ctx, const void* input, int n, int is_complex, const float* mother,
+                    int mother_size, const float* scales, int fn, int threads, unsigned flags, void* output,
+                    int out_type);
 /* Introspection (no reference counterpart): rows the plan produces and how many
  * of them the tensor-core engine runs (the rest run on the CUDA-core engine). */
 int fcwt_plan_stats(const fcwt_plan* plan, int* rows, int* tensor_core_rows);

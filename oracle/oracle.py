@@ -145,11 +145,13 @@ class Restatement:
         return sel, W
 
     def cwt_fp64(self, x, scales, fb: float, threads: int = 1, norm: bool = True,
-                 avx: bool = True, rows=None) -> np.ndarray:
+                 avx: bool = True, rows=None, mother=None) -> np.ndarray:
         """Float64 restatement of FCWT::cwt (src/fcwt/fcwt.cpp:447-529) with the
         reference's exact truncation, indices and stale-bin weights, and
-        float64 FFTs. Returns complex128 [fn, n], or [len(rows), n] for the
-        selected rows (ascending)."""
+        float64 FFTs. `mother` replaces the Morlet(fb) table by a caller's
+        frequency-domain table of N entries (the Wavelet::generate(N) result,
+        fcwt.cpp:504-505). Returns complex128 [fn, n], or [len(rows), n] for
+        the selected rows (ascending)."""
         x = np.asarray(x)
         n = x.size
         N = self.padded(n)
@@ -158,7 +160,8 @@ class Restatement:
         Ihat = np.fft.fft(xp)
         scales = np.ascontiguousarray(scales, np.float32)
         sel = list(range(scales.size)) if rows is None else sorted(int(r) for r in rows)
-        _, W = self.weights_rows(N, scales, threads, self.mother(fb, N), sel, avx)
+        table = self.mother(fb, N) if mother is None else np.ascontiguousarray(mother, np.float32)
+        _, W = self.weights_rows(N, scales, threads, table, sel, avx)
         half = N // 2
         out = np.zeros((len(sel), n), np.complex128)
         for k in range(len(sel)):
@@ -189,6 +192,8 @@ class Reference:
         L.ref_cwt.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float, _vp, ctypes.c_int,
                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]
         L.ref_find2power.restype = ctypes.c_int
+        L.ref_cwt_table.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, _vp]
 
     @staticmethod
     def available(path: str = REF_LIB_PATH) -> bool:
@@ -207,6 +212,18 @@ class Reference:
     def mother(self, fb: float, N: int) -> np.ndarray:
         out = np.zeros(N, np.float32)
         self.lib.ref_mother(fb, N, _ptr(out))
+        return out
+
+    def cwt_table(self, x, table, scales, threads: int = 1, norm: bool = True) -> np.ndarray:
+        """FCWT::cwt with a wavelet whose generate(N) returns `table`."""
+        x = np.asarray(x)
+        cplx = np.iscomplexobj(x)
+        xin = np.ascontiguousarray(x, np.complex64 if cplx else np.float32)
+        sc = np.ascontiguousarray(scales, np.float32)
+        t = np.ascontiguousarray(table, np.float32)
+        out = np.zeros((sc.size, xin.size), np.complex64)
+        self.lib.ref_cwt_table(_ptr(xin), xin.size, 1 if cplx else 0, _ptr(t), t.size, _ptr(sc), sc.size,
+                               int(threads), 1 if norm else 0, _ptr(out))
         return out
 
     def support(self, fb: float, scale: float) -> int:

@@ -13,6 +13,9 @@
 //   ref_wavelet     -> Morlet::getWavelet                      (src/fcwt/fcwt.cpp:86-105)
 //   ref_cwt         -> FCWT::cwt (real or complex input)       (src/fcwt/fcwt.cpp:447-548)
 //   ref_create_plan -> FCWT::create_FFT_optimization_plan      (src/fcwt/fcwt.cpp:313-374)
+//   ref_cwt_table   -> FCWT::cwt with a Wavelet subclass whose generate(N)
+//                      fills `mother` from a caller table (the reference's
+//                      Wavelet interface, src/fcwt/fcwt.h:67-79)
 #include "fcwt.h"
 
 #include <cstring>
@@ -61,6 +64,42 @@ void ref_cwt(const void* input, int n, int is_complex, float fb, const float* sc
     Scales s(&m, FCWT_LOGSCALES, fs, 1.0f, 2.0f, fn);
     std::memcpy(s.scales, scales, sizeof(float) * (size_t)fn);
     FCWT f(&m, threads, optplans != 0, norm != 0);
+    if (is_complex) {
+        f.cwt((std::complex<float>*)input, n, (std::complex<float>*)output, &s);
+    } else {
+        f.cwt((float*)input, n, (std::complex<float>*)output, &s);
+    }
+    free(s.scales);
+}
+
+// A wavelet given by its frequency-domain table (single-sided, real), as a
+// user subclass of the reference's Wavelet would provide it.
+class TableWavelet : public Wavelet {
+public:
+    TableWavelet(const float* t, int n) : table(t), size(n) {
+        imag_frequency = false;
+        doublesided = false;
+        four_wavelen = 1.0f;
+        mother = nullptr;
+    }
+    ~TableWavelet() { free(mother); }
+    void generate(int n) override {
+        free(mother);
+        mother = (float*)malloc(sizeof(float) * (size_t)n);
+        for (int i = 0; i < n; i++) mother[i] = i < size ? table[i] : 0.0f;
+        width = n;
+    }
+    const float* table;
+    int size;
+};
+
+void ref_cwt_table(const void* input, int n, int is_complex, const float* table, int table_size,
+                   const float* scales, int fn, int threads, int norm, void* output) {
+    TableWavelet w(table, table_size);
+    Morlet m(2.0f);
+    Scales s(&m, FCWT_LOGSCALES, 1000, 1.0f, 2.0f, fn);
+    std::memcpy(s.scales, scales, sizeof(float) * (size_t)fn);
+    FCWT f(&w, threads, false, norm != 0);
     if (is_complex) {
         f.cwt((std::complex<float>*)input, n, (std::complex<float>*)output, &s);
     } else {
