@@ -186,7 +186,8 @@ template <int KP, int OT>
 __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                        const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                        const float2* __restrict__ twhi, const float2* __restrict__ t2, uint32_t tmem,
-                                       uint32_t mbar_h, uint32_t& phase, float* s_red) {
+                                       uint32_t mbar_h, uint32_t& phase, float* s_red, int* next_idx,
+                                       RowDesc* next_R, SigDesc* next_S) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -284,7 +285,22 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int amax = (n + M - 1) / M;  // stripes a that hold output samples
     // the halves run the same per-group sequence; starting half 1 a little later
     // keeps their DFT (issue-bound) and staging/store (SMEM-bound) phases apart
-    if (h == 1) __nanosleep(500);
+    if (h == 1 && wl == 7 && lane == 0) {
+        // claim the CTA's next row now and pull its weights and spectrum window into L2
+        const int i = (int)atomicAdd(P.counter, 1u);
+        *next_idx = i;
+        if (i < P.n_list) {
+            *next_R = P.rows[P.row_list[i]];
+            *next_S = P.sigs[next_R->sig];
+            const unsigned wb = (unsigned)(kP2 * next_R->kp) * 4u;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.wts + next_R->woff), "r"(wb) : "memory");
+            const int Nn = 1 << next_S->log2N;
+            const int xe = min(kP2 * next_R->kp, Nn - next_R->L);
+            if (xe > 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next_S->X + next_R->L),
+                             "r"((unsigned)xe * 8u) : "memory");
+        }
+    }
     while (g < ng) {
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
@@ -391,10 +407,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float2* twhi_s = reinterpret_cast<float2*>(sm + kTcOffTwhi);
     __shared__ __align__(8) unsigned long long s_mbar[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_idx;
+    __shared__ int s_idx[2];
     __shared__ int s_log2N;
-    __shared__ RowDesc s_R;
-    __shared__ SigDesc s_S;
+    __shared__ RowDesc s_R[2];
+    __shared__ SigDesc s_S[2];
     __shared__ float s_red[kTcThreads / 32];
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -424,34 +440,40 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t mbar_h = smem_u32(&s_mbar[h]);
     uint32_t phase = 0;
 
-    for (;;) {
-        if (tid == 0) {
-            const int i = (int)atomicAdd(P.counter, 1u);
-            s_idx = i;
-            if (i < P.n_list) {
-                s_R = P.rows[P.row_list[i]];
-                s_S = P.sigs[s_R.sig];
-            }
+    if (tid == 0) {
+        const int i = (int)atomicAdd(P.counter, 1u);
+        s_idx[0] = i;
+        if (i < P.n_list) {
+            s_R[0] = P.rows[P.row_list[i]];
+            s_S[0] = P.sigs[s_R[0].sig];
         }
-        __syncthreads();
-        if (s_idx >= P.n_list) break;
-        const int log2N = s_S.log2N;
+    }
+    __syncthreads();
+    int sl = 0;
+    for (;;) {
+        if (s_idx[sl] >= P.n_list) break;
+        const RowDesc& R = s_R[sl];
+        const SigDesc& S = s_S[sl];
+        const int log2N = S.log2N;
         const int M = 1 << (log2N - kLog2P2);
         if (log2N != s_log2N) {
-            for (int j = tid; j < kP2; j += kTcThreads) twlo[j] = s_S.tw[j];
+            for (int j = tid; j < kP2; j += kTcThreads) twlo[j] = S.tw[j];
             if (M <= kTcTwhiSmem)
-                for (int j = tid; j < M; j += kTcThreads) twhi_s[j] = s_S.tw[kP2 + j];
+                for (int j = tid; j < M; j += kTcThreads) twhi_s[j] = S.tw[kP2 + j];
         }
         __syncthreads();
         if (tid == 0) s_log2N = log2N;
-        const float2* twhi = M <= kTcTwhiSmem ? twhi_s : s_S.tw + kP2;
-        if (s_R.kp > 8)
-            row_tc<16, OT>(P, &omap, s_R, s_S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red);
+        const float2* twhi = M <= kTcTwhiSmem ? twhi_s : S.tw + kP2;
+        if (R.kp > 8)
+            row_tc<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                           &s_R[sl ^ 1], &s_S[sl ^ 1]);
         else
-            row_tc<8, OT>(P, &omap, s_R, s_S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red);
+            row_tc<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                          &s_R[sl ^ 1], &s_S[sl ^ 1]);
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
+        sl ^= 1;
     }
     if ((tid & 31) == 0 && ((tid >> 5) & 7) >= 4 && P.tma_store) bulk_wait_all();
     tc_fence_before();
