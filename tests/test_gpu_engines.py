@@ -193,3 +193,23 @@ def test_power_and_db_epilogues(fcwt, oracle, ctx, mode, n):
     assert np.linalg.norm(pw - ref) / np.linalg.norm(ref) < 2e-5
     mask = ref > 1e-6 * ref.max()
     assert np.max(np.abs(db[mask] - 10 * np.log10(ref[mask]))) < 1e-3
+
+
+@pytest.mark.parametrize("mode", ["tensor_cores", "cuda_cores"])
+def test_maximum_padded_length(fcwt, oracle, ctx, mode):
+    """n just above 2^22 (N = 2^23, the largest supported): 8192 columns per
+    row, the w_M table read from global memory, 1024 column groups."""
+    from fcwt_b200 import _lib
+
+    ctx.set_engine(_lib.FCWT_ENGINE_TENSOR_CORES if mode == "tensor_cores" else _lib.FCWT_ENGINE_CUDA_CORES)
+    n = (1 << 22) + 1000
+    rng = np.random.default_rng(23)
+    x = (rng.standard_normal(n) + np.sin(np.arange(n) * 1e-3)).astype(np.float32)
+    sc = oracle.scales(LOGSCALES, 1000, 0.5, 1.5, 6)  # windows of <= 16 blocks of 1024 bins
+    p = fcwt.Plan(n, sc, fb=2.0, threads=1, norm=True)
+    if mode == "tensor_cores":
+        assert p.stats()["tensor_core_rows"] == 6
+    out = np.zeros((6, n), np.complex64)
+    p.execute(x, out)
+    p.close()
+    assert rel_l2(out, oracle.cwt_fp64(x, sc, 2.0, 1, True)) < TOL
