@@ -41,9 +41,9 @@ FS = 1000
 F0, F1, FN = 1.0, 101.0, 3000
 SIGMA = 2.0
 # DRAM bytes (read + write) of one k_row_tc launch of this workload: ncu
-# dram__bytes_read.sum 149.06 MB + dram__bytes_write.sum 2.35 GB (one-pass
+# dram__bytes_read.sum 282.39 MB + dram__bytes_write.sum 2.35 GB (one-pass
 # capture of the full-size launch; profiles/k_row_tc_cwt100k_x3000.md)
-TRAFFIC_PER_LAUNCH = 149.06e6 + 2.35e9
+TRAFFIC_PER_LAUNCH = 282.39e6 + 2.35e9
 WORKLOAD = "cwt_100k_x_3000: real f32 n=100000 (N=131072) fs=1000, Morlet sigma=2, LINFREQS 1-101 Hz fn=3000, complex64 out"
 
 
