@@ -18,8 +18,8 @@
 // One persistent CTA of 16 warps per SM takes rows from a queue. Per row:
 //   pre-pass  all warps evaluate Z on the window, scale it by 2^e
 //             (max |Z| 2^e in [2^14, 2^15)), split it into FP16 hi + lo and
-//             store it in tensor memory as the A operand: tile t (k2 in
-//             [128 t, 128 t + 128)) is lanes 0..127, columns
+//             store it in tensor memory as the A operand: tile t is lanes
+//             0..127 (lane 32 q + l holds k2 = l + 32 (8 q + t)), columns
 //             [(2t + p) Kp, +Kp) for p = hi, lo; column k1 holds (re, im) as a
 //             half2, i.e. GEMM K index 2 k1 + {0, 1}.
 //   groups    the two halves of the CTA (8 warps each) take alternating groups
@@ -31,6 +31,8 @@
 //             column tiles; one warp per column runs the 1024-point DFT;
 //             swizzled staging and TMA tensor stores of [256 a][8 c] boxes.
 //             The MMAs of the half's next group are issued before its DFT.
+//             For BF16 / FP16 outputs the column DFTs run on the tensor cores
+//             as well (two radix-32 GEMM stages, row_tc_dft).
 // Tensor memory: 512 columns per CTA (A: 0..255, accumulators of half h:
 // 256 + 128 h + 16 t for tile t).
 #include "fcwt_dev.cuh"
@@ -50,8 +52,11 @@ constexpr int kTcOffTwhi = kTcOffT2 + kP2 * 8;
 constexpr int kTcOffB = kTcOffTwhi + kTcTwhiSmem * 8;
 constexpr int kTcBBytes = 16 * 2 * kTcMaxKp * 2;  // one B operand (16 rows x 2Kp halves), 1 KB
 constexpr int kTcOffTg = kTcOffB + 2 * 2 * kTcBBytes;
-constexpr int kTcOffEnd = kTcOffTg + 2 * 32 * 8;
+constexpr int kTcOffW32 = (kTcOffTg + 2 * 32 * 8 + 1023) & ~1023;  // DFT-32 matrix, 128B-swizzled
+constexpr int kTcW32Bytes = 64 * 128;
+constexpr int kTcOffEnd = kTcOffW32 + kTcW32Bytes;
 constexpr size_t kTcSmemBytes = (size_t)kTcOffEnd + 1024;
+constexpr int kTcStageBlock = 128 * 128;  // one 128-row block of a DFT-stage operand (16 KB)
 static_assert(4 * kBoxBytes == kTcGbufBytes, "staging boxes fill one G buffer");
 
 // Instruction descriptor: D f32, A/B f16, both K-major, N = 16, M = 128.
@@ -72,6 +77,27 @@ __device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a, uint64_t bdesc, u
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
         "r"(a), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+// DFT stages: D f32, A/B f16, both K-major, N = 64, M = 128.
+constexpr uint32_t kTcIdescDft = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+// Byte offset of byte `kb` of row r in a K-major operand with 128-byte rows in
+// the 128B-swizzled layout (8-row atoms of 1 KB; 16-byte chunk index XOR row % 8).
+__device__ __forceinline__ uint32_t sw128_off(int r, int kb) {
+    return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((kb >> 4) ^ r) & 7) << 4) + (kb & 15));
+}
+// Shared-memory matrix descriptor of a 128B-swizzled K-major operand (atoms
+// 1 KB apart along M/N); K steps of 16 elements advance the address by 32 B.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 __device__ __forceinline__ void mma_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
@@ -182,6 +208,90 @@ __device__ __forceinline__ void issue_group(int t, uint32_t tmem, uint32_t dcol,
     }
 }
 
+// Pre-pass of a row: Z on the window, scaled by 2^e (max |Z| 2^e in
+// [2^14, 2^15)) and split into FP16 hi + lo, into tensor memory as the A
+// operand (tile t, lane 32 q + l holds k2 = l + 32 (8 q + t)). Returns 2^-e.
+template <int KP>
+__device__ __forceinline__ float tc_prepass(const TcParams& P, const RowDesc& R, const SigDesc& S, uint32_t tmem,
+                                            float* s_red) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int qd = warp & 3;
+    const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+    const float* __restrict__ wrow = P.wts + R.woff;
+    const int tsel = warp >> 2;  // this warp's tiles: tsel, tsel + 4
+    float2 z[2][KP];
+    float mx = 0.0f;
+#pragma unroll
+    for (int ti = 0; ti < 2; ti++) {
+        const int k2 = lane + 32 * (8 * qd + tsel + 4 * ti);
+#pragma unroll
+        for (int k1 = 0; k1 < KP; k1++) {
+            const int q = R.L + k2 + kP2 * k1;
+            const float m = __ldg(wrow + k2 + kP2 * k1);
+            const float2 xv = (q >= R.lo && q < R.hi) ? __ldg(S.X + q) : make_float2(0.0f, 0.0f);
+            const float2 v = make_float2(xv.x * m, xv.y * m);
+            z[ti][k1] = v;
+            mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) s_red[warp] = mx;
+    __syncthreads();
+    mx = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kTcThreads / 32; w++) mx = fmaxf(mx, s_red[w]);
+    int ex = 0;
+    if (mx > 0.0f) frexpf(mx, &ex);
+    const int e2 = max(-126, min(126, 15 - ex));
+    const float scale = ldexpf(1.0f, e2);
+#pragma unroll
+    for (int ti = 0; ti < 2; ti++) {
+        const int t = tsel + 4 * ti;
+        uint32_t hv[KP], lv[KP];
+#pragma unroll
+        for (int k1 = 0; k1 < KP; k1++) {
+            const float a = z[ti][k1].x * scale;
+            const float b = z[ti][k1].y * scale;
+            const __half2 hh = __floats2half2_rn(a, b);
+            const float2 hf = __half22float2(hh);
+            hv[k1] = h2bits(hh);
+            lv[k1] = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+        }
+        const uint32_t ta = tmem + lane_base + (uint32_t)(2 * t * KP);
+#pragma unroll
+        for (int q = 0; q < KP / 8; q++) {
+            tmem_st8(ta + 8u * q, hv + 8 * q);
+            tmem_st8(ta + KP + 8u * q, lv + 8 * q);
+        }
+    }
+    tmem_wait_st();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return ldexpf(1.0f, -e2);
+}
+
+// Claims the CTA's next row from the queue into the other row slot and pulls
+// its weights and spectrum window into L2.
+__device__ __forceinline__ void tc_claim_next(const TcParams& P, int* next_idx, RowDesc* next_R, SigDesc* next_S) {
+    const int i = (int)atomicAdd(P.counter, 1u);
+    *next_idx = i;
+    if (i < P.n_list) {
+        *next_R = P.rows[P.row_list[i]];
+        *next_S = P.sigs[next_R->sig];
+        const unsigned wb = (unsigned)(kP2 * next_R->kp) * 4u;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.wts + next_R->woff), "r"(wb) : "memory");
+        const int Nn = 1 << next_S->log2N;
+        const int xe = min(kP2 * next_R->kp, Nn - next_R->L);
+        if (xe > 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next_S->X + next_R->L),
+                         "r"((unsigned)xe * 8u) : "memory");
+    }
+}
+
 template <int KP, int OT>
 __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                        const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
@@ -202,63 +312,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int n = S.n;
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
-    // ---- pre-pass: Z on the window into tensor memory (split FP16)
-    float scale, inv;
-    {
-        const float* __restrict__ wrow = P.wts + R.woff;
-        const int tsel = warp >> 2;  // this warp's tiles: tsel, tsel + 4
-        float2 z[2][KP];
-        float mx = 0.0f;
-#pragma unroll
-        for (int ti = 0; ti < 2; ti++) {
-            const int k2 = 128 * (tsel + 4 * ti) + 32 * qd + lane;
-#pragma unroll
-            for (int k1 = 0; k1 < KP; k1++) {
-                const int q = R.L + k2 + kP2 * k1;
-                const float m = __ldg(wrow + k2 + kP2 * k1);
-                const float2 xv = (q >= R.lo && q < R.hi) ? __ldg(S.X + q) : make_float2(0.0f, 0.0f);
-                const float2 v = make_float2(xv.x * m, xv.y * m);
-                z[ti][k1] = v;
-                mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) s_red[warp] = mx;
-        __syncthreads();
-        mx = 0.0f;
-#pragma unroll
-        for (int w = 0; w < kTcThreads / 32; w++) mx = fmaxf(mx, s_red[w]);
-        int ex = 0;
-        if (mx > 0.0f) frexpf(mx, &ex);
-        const int e2 = max(-126, min(126, 15 - ex));
-        scale = ldexpf(1.0f, e2);
-        inv = ldexpf(1.0f, -e2);
-#pragma unroll
-        for (int ti = 0; ti < 2; ti++) {
-            const int t = tsel + 4 * ti;
-            uint32_t hv[KP], lv[KP];
-#pragma unroll
-            for (int k1 = 0; k1 < KP; k1++) {
-                const float a = z[ti][k1].x * scale;
-                const float b = z[ti][k1].y * scale;
-                const __half2 hh = __floats2half2_rn(a, b);
-                const float2 hf = __half22float2(hh);
-                hv[k1] = h2bits(hh);
-                lv[k1] = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
-            }
-            const uint32_t ta = tmem + lane_base + (uint32_t)(2 * t * KP);
-#pragma unroll
-            for (int q = 0; q < KP / 8; q++) {
-                tmem_st8(ta + 8u * q, hv + 8 * q);
-                tmem_st8(ta + KP + 8u * q, lv + 8 * q);
-            }
-        }
-        tmem_wait_st();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-    }
+    const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
 
     // ---- column groups
     const int ng = M / kTcCols;
@@ -285,22 +339,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int amax = (n + M - 1) / M;  // stripes a that hold output samples
     // the halves run the same per-group sequence; starting half 1 a little later
     // keeps their DFT (issue-bound) and staging/store (SMEM-bound) phases apart
-    if (h == 1 && wl == 7 && lane == 0) {
-        // claim the CTA's next row now and pull its weights and spectrum window into L2
-        const int i = (int)atomicAdd(P.counter, 1u);
-        *next_idx = i;
-        if (i < P.n_list) {
-            *next_R = P.rows[P.row_list[i]];
-            *next_S = P.sigs[next_R->sig];
-            const unsigned wb = (unsigned)(kP2 * next_R->kp) * 4u;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.wts + next_R->woff), "r"(wb) : "memory");
-            const int Nn = 1 << next_S->log2N;
-            const int xe = min(kP2 * next_R->kp, Nn - next_R->L);
-            if (xe > 0)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(next_S->X + next_R->L),
-                             "r"((unsigned)xe * 8u) : "memory");
-        }
-    }
+    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
     while (g < ng) {
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
@@ -312,7 +351,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             uint32_t r[16];
             tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
             tmem_wait_ld();
-            const int k2 = 128 * (tb + tt) + 32 * qd + lane;
+            const int k2 = lane + 32 * (8 * qd + tb + tt);
             float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], inv));
             const float2 stp = twlo[k2];
 #pragma unroll
@@ -328,7 +367,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
-            const int k2 = 128 * (tb + tt) + 32 * qd + lane;
+            const int k2 = lane + 32 * (8 * qd + tb + tt);
 #pragma unroll
             for (int j = 0; j < kTcCols; j++) gbuf[j * kP2 + k2] = gv[tt][j];
         }
@@ -397,6 +436,214 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     }
 }
 
+// The 16-bit outputs (BF16 / FP16 pairs) also run the column DFTs on the
+// tensor cores. With k2 = kl + 32 kb and a = a1 + 32 a2,
+//     H[c][kl][a1]     = sum_kb G[c][kl + 32 kb] w_32^{a1 kb}                 (stage 1)
+//     y[c + M (a1 + 32 a2)] = sum_kl H[c][kl][a1] w_1024^{a1 kl} w_32^{a2 kl}  (stage 2)
+// Each stage is a real GEMM [256 x 64] x [64 x 64] (complex values as
+// (re, im) pairs, FP16 operands, FP32 accumulation) against the DFT-32
+// matrix W / 32 in SMEM, both operands K-major and 128B-swizzled. The scale
+// factors are fixed powers of two: |G| / Kp <= 2^15.5 and a stage cannot grow
+// the largest value (the 1/32 in W), so no FP16 operand overflows; the output
+// scale 2^-e Kp 1024 is applied once at the end. Row orders: stage 1, block
+// c / 4, row 32 (c % 4) + kl (each thread writes 16-byte pieces of four kb);
+// stage 2, block a1 / 16, row 8 (a1 % 16) + c, so that a warp's stage-2
+// accumulators are [4 a][8 c] tiles of the output staging. Both stages reuse
+// the half's 128 accumulator columns; the phase-1 MMAs of the half's next group
+// are issued once the stage-2 results are in registers.
+__device__ __forceinline__ void issue_dft_stage(uint32_t d, uint32_t a, uint32_t w) {
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int kb = 0; kb < 4; kb++)
+            mma_ss(d + 64u * m, umma_desc_sw128(a + (uint32_t)(kTcStageBlock * m) + 32u * kb),
+                   umma_desc_sw128(w + 32u * kb), kTcIdescDft, kb != 0 ? 1u : 0u);
+}
+
+template <int KP, int OT>
+__device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
+                                           const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
+                                           const float2* __restrict__ twhi, const float2* __restrict__ t2,
+                                           uint32_t tmem, uint32_t mbar_h, uint32_t& phase, uint32_t mbar2_h,
+                                           uint32_t& phase2, float* s_red, int* next_idx, RowDesc* next_R,
+                                           SigDesc* next_S) {
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int h = warp >> 3;
+    const int ht = tid & 255;
+    const int wl = warp & 7;
+    const int qd = warp & 3;
+    const int log2N = S.log2N;
+    const int N = 1 << log2N;
+    const int M = N >> kLog2P2;
+    const unsigned Nm = (unsigned)N - 1u;
+    const int n = S.n;
+    const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+
+    const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
+    const float s1 = 1.0f / (float)KP;
+    const float fin = inv * (float)(KP * 1024);
+
+    const int ng = M / kTcCols;
+    unsigned char* abuf = sm + h * kTcGbufBytes;        // DFT-stage A operand, 32 KB
+    unsigned char* stage = abuf + kTcGbufBytes / 2;     // output staging, 32 KB
+    unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
+    unsigned char* blo = bhi + kTcBBytes;
+    float2* tg = reinterpret_cast<float2*>(sm + kTcOffTg) + 32 * h;
+    const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
+    const uint32_t abuf_a = smem_u32(abuf), w32_a = smem_u32(sm + kTcOffW32);
+    const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
+    const bool tma = P.tma_store != 0 && R.out_buf == 0;
+    void* outb = P.outs[R.out_buf];
+    int g = h;
+    if (g < ng) {
+        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        fence_proxy_async_smem();
+        half_bar(h);
+        if (lane == 0) {
+            tc_fence_after();
+            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            mma_commit(mbar_h);
+        }
+    }
+    const int tb = (wl >> 2) * 4;      // this warp drains phase-1 tiles tb .. tb + 3
+    const int amax = (n + M - 1) / M;  // stripes a that hold output samples
+    // stage-1 operand: this thread's rows 32 (j % 4) + lane of block j / 4, bytes 4 kb for kb = 8 qd + tb + 0..3
+    const uint32_t a1_off = (uint32_t)((lane >> 3) * 1024 + (lane & 7) * 128 + ((((2 * qd + (tb >> 2)) ^ lane) & 7) << 4));
+    // stage-2 operand: row 8 (a1 % 16) + wl of block a1 / 16, bytes 4 lane
+    const uint32_t a2_off = (uint32_t)(wl * 128 + ((((lane >> 2) ^ wl) & 7) << 4) + (lane & 3) * 4);
+    // stage-2 accumulators of this thread: a1 = 16 (wl / 4) + 4 qd + lane / 8, column c = lane % 8
+    const int my_a1 = 16 * (wl >> 2) + 4 * qd + (lane >> 3);
+    const int my_c = lane & 7;
+    const uint32_t dsrc = dcol + lane_base + 64u * (uint32_t)(wl >> 2);
+    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
+    while (g < ng) {
+        mbar_wait(mbar_h, phase, P.err);
+        phase ^= 1u;
+        tc_fence_after();
+        const int c0 = g * kTcCols;
+        {
+            uint32_t pk[kTcCols][4];
+#pragma unroll
+            for (int tt = 0; tt < 4; tt++) {
+                uint32_t r[16];
+                tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
+                tmem_wait_ld();
+                const int k2 = lane + 32 * (8 * qd + tb + tt);
+                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], s1));
+                const float2 stp = twlo[k2];
+#pragma unroll
+                for (int j = 0; j < kTcCols; j++) {
+                    const float2 v = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
+                    pk[j][tt] = h2bits(__floats2half2_rn(v.x, v.y));
+                    if (j + 1 < kTcCols) w = cmul(w, stp);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kTcCols; j++)
+                *reinterpret_cast<uint4*>(abuf + (j >> 2) * kTcStageBlock + (j & 3) * 4096 + a1_off) =
+                    make_uint4(pk[j][0], pk[j][1], pk[j][2], pk[j][3]);
+        }
+        tc_fence_before();
+        fence_proxy_async_smem();
+        half_bar(h);  // phase-1 accumulators drained; stage-1 operand in SMEM
+        if (wl == 0 && lane == 0) {
+            tc_fence_after();
+            issue_dft_stage(dcol, abuf_a, w32_a);
+            mma_commit(mbar2_h);
+        }
+        const int gn = g + 2;
+        if (gn < ng) {
+            build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+            fence_proxy_async_smem();
+        }
+        mbar_wait(mbar2_h, phase2, P.err);
+        phase2 ^= 1u;
+        tc_fence_after();
+        // stage-1 results of column c = wl, kl = lane: twiddle, stage-2 operand
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t r[16];
+            tmem_ld16(dsrc + 16u * q, r);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int a1 = 8 * q + i;
+                const float2 v = cmul(make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])),
+                                      t2[a1 * 32 + lane]);
+                *reinterpret_cast<uint32_t*>(abuf + (a1 >> 4) * kTcStageBlock + (a1 & 15) * 1024 + a2_off) =
+                    h2bits(__floats2half2_rn(v.x, v.y));
+            }
+        }
+        tc_fence_before();
+        fence_proxy_async_smem();
+        half_bar(h);  // stage-1 accumulators drained; stage-2 operand in SMEM
+        if (wl == 0 && lane == 0) {
+            tc_fence_after();
+            issue_dft_stage(dcol, abuf_a, w32_a);
+            mma_commit(mbar2_h);
+        }
+        mbar_wait(mbar2_h, phase2, P.err);
+        phase2 ^= 1u;
+        tc_fence_after();
+        uint32_t yv[32];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t r[16];
+            tmem_ld16(dsrc + 16u * q, r);
+            tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                yv[8 * q + i] = pack16<OT>(
+                    make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
+        }
+        tc_fence_before();
+        if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
+        half_bar(h);  // accumulators free for the next group; staging free
+        if (lane == 0 && gn < ng) {
+            tc_fence_after();
+            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            mma_commit(mbar_h);
+        }
+#pragma unroll
+        for (int a2 = 0; a2 < 32; a2++) {
+            const int a = my_a1 + 32 * a2;
+            if (a < amax) *reinterpret_cast<unsigned*>(stage + stage16_off(a, my_c)) = yv[a2];
+        }
+        const long long row0 = R.out_off + c0;
+        constexpr int box_bytes = kBoxBytes / 2;
+        if (tma) {
+            fence_proxy_async_smem();
+            half_bar(h);
+            const int n_full = n / M;
+            if (lane == 0 && wl >= 4) {
+                const int j = wl - 4;
+                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
+                bulk_commit();
+            }
+            const int tail = n - n_full * M;
+            if (ht < kTcCols && c0 + ht < tail && n_full < kP2) {
+                const long long idx = row0 + ht + (long long)M * n_full;
+                __stcs(reinterpret_cast<unsigned*>(outb) + idx,
+                       *reinterpret_cast<const unsigned*>(stage + stage16_off(n_full, ht)));
+            }
+        } else {
+            half_bar(h);
+            for (int idx = ht; idx < kTcCols * kP2; idx += 256) {
+                const int w = idx & (kTcCols - 1);
+                const int a = idx >> 3;
+                if (c0 + w + (long long)M * a < n) {
+                    const long long o = row0 + w + (long long)M * a;
+                    __stcs(reinterpret_cast<unsigned*>(outb) + o,
+                           *reinterpret_cast<const unsigned*>(stage + stage16_off(a, w)));
+                }
+            }
+        }
+        g = gn;
+    }
+}
+
 template <int OT>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_row_tc(const __grid_constant__ TcParams P, const __grid_constant__ CUtensorMap omap) {
@@ -406,6 +653,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float2* t2 = reinterpret_cast<float2*>(sm + kTcOffT2);
     float2* twhi_s = reinterpret_cast<float2*>(sm + kTcOffTwhi);
     __shared__ __align__(8) unsigned long long s_mbar[2];
+    __shared__ __align__(8) unsigned long long s_mbar2[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_idx[2];
     __shared__ int s_log2N;
@@ -422,9 +670,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         sincospi(2.0 * (double)((a * l) & 1023) / 1024.0, &s, &c);
         t2[j] = make_float2((float)c, (float)s);
     }
+    if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
+        // W / 32 for the DFT stages: row n = 2 a + {re, im}, K index 2 k + {re, im}
+        unsigned char* w32 = sm + kTcOffW32;
+        for (int j = tid; j < 64 * 64; j += kTcThreads) {
+            const int nr = j >> 6, k = j & 63;
+            double s, c;
+            sincospi((double)(((nr >> 1) * (k >> 1)) & 31) / 16.0, &s, &c);
+            const float cv = (float)c * (1.0f / 32.0f), sv = (float)s * (1.0f / 32.0f);
+            const float v = (nr & 1) == 0 ? ((k & 1) == 0 ? cv : -sv) : ((k & 1) == 0 ? sv : cv);
+            *reinterpret_cast<__half*>(w32 + sw128_off(nr, 2 * k)) = __float2half_rn(v);
+        }
+        fence_proxy_async_smem();
+    }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[1])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar2[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar2[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_log2N = -1;
     }
@@ -438,7 +701,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     const uint32_t tmem = s_tmem;
     const uint32_t mbar_h = smem_u32(&s_mbar[h]);
-    uint32_t phase = 0;
+    const uint32_t mbar2_h = smem_u32(&s_mbar2[h]);
+    uint32_t phase = 0, phase2 = 0;
 
     if (tid == 0) {
         const int i = (int)atomicAdd(P.counter, 1u);
@@ -464,12 +728,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
         if (tid == 0) s_log2N = log2N;
         const float2* twhi = M <= kTcTwhiSmem ? twhi_s : S.tw + kP2;
-        if (R.kp > 8)
-            row_tc<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
-                           &s_R[sl ^ 1], &s_S[sl ^ 1]);
-        else
-            row_tc<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
-                          &s_R[sl ^ 1], &s_S[sl ^ 1]);
+        if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
+            if (R.kp > 8)
+                row_tc_dft<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
+                                   &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
+            else
+                row_tc_dft<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
+                                  &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
+        } else {
+            if (R.kp > 8)
+                row_tc<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                               &s_R[sl ^ 1], &s_S[sl ^ 1]);
+            else
+                row_tc<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                              &s_R[sl ^ 1], &s_S[sl ^ 1]);
+        }
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
