@@ -44,6 +44,15 @@ SIGMA = 2.0
 # dram__bytes_read.sum 282.39 MB + dram__bytes_write.sum 2.35 GB (one-pass
 # capture of the full-size launch; profiles/k_row_tc_cwt100k_x3000.md)
 TRAFFIC_PER_LAUNCH = 282.39e6 + 2.35e9
+
+# --out choices: (constant in fcwt_b200, trailing shape, torch dtype, bytes per point)
+OUT_TYPES = {
+    "complex64": ("FCWT_OUT_C64", (), "complex64", 8),
+    "bf16": ("FCWT_OUT_BF16", (2,), "bfloat16", 4),
+    "f16": ("FCWT_OUT_F16", (2,), "float16", 4),
+    "power": ("FCWT_OUT_POWER", (), "float32", 4),
+    "db": ("FCWT_OUT_DB", (), "float32", 4),
+}
 WORKLOAD = "cwt_100k_x_3000: real f32 n=100000 (N=131072) fs=1000, Morlet sigma=2, LINFREQS 1-101 Hz fn=3000, complex64 out"
 
 
@@ -200,6 +209,9 @@ def main():
     ap.add_argument("--fn", type=int, default=FN,
                     help="number of rows; values other than 3000 are for profiling captures only")
     ap.add_argument("--no-forms", action="store_true", help="skip the BF16-output form of the default workload")
+    ap.add_argument("--out", default="complex64", choices=list(OUT_TYPES),
+                    help="output type of the timed transform; values other than complex64 are for profiling "
+                         "captures of the other epilogues (no forms then)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "grad", "long"],
                     help="plain: the 100k x 3000 transform (default); batched: 384 uneven channels, one "
                          "persistent launch vs a per-channel loop; grad: differentiable transform, forward + "
@@ -241,12 +253,16 @@ def main():
     N = 1 << _lib.load().fcwt_find2power(N_SAMPLES)
     xd = torch.from_numpy(x).to(f"cuda:{dev}")
     out = torch.empty((fn, N_SAMPLES), dtype=torch.complex64, device=f"cuda:{dev}")
+    out_code, out_shape, out_dtype, out_bytes = OUT_TYPES[args.out]
+    out_t = out if args.out == "complex64" else torch.empty((fn, N_SAMPLES) + out_shape, dtype=getattr(torch, out_dtype),
+                                                            device=f"cuda:{dev}")
+    out_type = getattr(fcwt, out_code)
     stream = torch.cuda.current_stream(dev)
     ctx = plan.ctx
 
     # warm-up
     for _ in range(args.warmup):
-        plan.execute(xd, out, stream=stream)
+        plan.execute(xd, out_t, out_type=out_type, stream=stream)
     torch.cuda.synchronize(dev)
     ctx.synchronize()
 
@@ -263,7 +279,7 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        plan.execute(xd, out, stream=stream)
+        plan.execute(xd, out_t, out_type=out_type, stream=stream)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     if dist:
@@ -308,7 +324,7 @@ def main():
 
     # ---- BF16-output form of the same workload (half the output bytes)
     forms = None
-    if rank == 0 and world == 1 and not args.no_forms:
+    if rank == 0 and world == 1 and not args.no_forms and args.out == "complex64":
         outb = torch.empty((fn, N_SAMPLES, 2), dtype=torch.bfloat16, device=f"cuda:{dev}")
         for _ in range(args.warmup):
             plan.execute(xd, outb, out_type=fcwt.FCWT_OUT_BF16, stream=stream)
@@ -374,16 +390,16 @@ def main():
              "k_row_engine" if st["tensor_core_rows"] == 0 else "k_row_tc + k_row_engine")
     # DRAM bytes of one launch of the row kernel (read + write), from the ncu
     # capture summarised in profiles/ (same workload); per launch like `achieved`
-    traffic = TRAFFIC_PER_LAUNCH if (fn == FN and kname == "k_row_tc") else None
-    algo = algorithmic_bytes(N_SAMPLES, fn, N)
+    traffic = TRAFFIC_PER_LAUNCH if (fn == FN and kname == "k_row_tc" and args.out == "complex64") else None
+    algo = algorithmic_bytes(N_SAMPLES, fn, N, out_bytes)
     achieved = algo / (eng_avg / 1e3) / 1e9
     line = {
         "metric": "scalogram points/s", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD if fn == FN else WORKLOAD.replace("fn=3000", f"fn={fn}"),
+        "config": {"workload": WORKLOAD.replace("fn=3000", f"fn={fn}").replace("complex64 out", f"{args.out} out"),
                    "n": N_SAMPLES, "N": N, "fn": fn, "fs": FS, "f0": F0, "f1": F1,
-                   "sigma": SIGMA, "scaling": "LINFREQS", "threads_param": 1, "out": "complex64",
+                   "sigma": SIGMA, "scaling": "LINFREQS", "threads_param": 1, "out": args.out,
                    "l2": "each step writes a 2.4 GB output (> 126 MB L2); no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -122,21 +122,24 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
 }
 
 // Bounded wait for phase `parity` of an mbarrier (gives up after
-// kWaitLimitNs, recording kErrWaitTimeout).
+// kWaitLimitNs, recording kErrWaitTimeout). Each try_wait may suspend the
+// thread until the phase completes, for at most kTrySuspendNs, so that waiting
+// warps do not take issue slots from the working ones.
+constexpr uint32_t kTrySuspendNs = 20000;
 __device__ bool mbar_wait(uint32_t mbar, uint32_t parity, int* err) {
     unsigned long long t0 = 0;
     for (unsigned it = 0;; it++) {
         uint32_t done;
         asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(mbar), "r"(parity)
+            : "r"(mbar), "r"(parity), "r"(kTrySuspendNs)
             : "memory");
         if (done) return true;
         if (it == 0) {
             t0 = global_ns();
-        } else if ((it & 63u) == 0 && global_ns() - t0 > kWaitLimitNs) {
+        } else if ((it & 7u) == 0 && global_ns() - t0 > kWaitLimitNs) {
             atomicOr(err, kErrWaitTimeout);
             return false;
         }
@@ -168,7 +171,7 @@ __device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, floa
 // K index 2 k1 + {re, im}; byte offset of element (n, k) in the canonical
 // K-major layout: (k / 16) * 512 + (n / 8) * 256 + ((k / 8) % 2) * 128 +
 // (n % 8) * 16 + (k % 8) * 2.
-template <int KP>
+template <int KP, bool LO = true>
 __device__ __forceinline__ void build_b(float2* __restrict__ tg, int g, int ht, int M, unsigned Nm, int L, const float2* __restrict__ twlo,
                                         const float2* __restrict__ twhi, unsigned char* bhi, unsigned char* blo) {
     if (ht >= 224) tg[ht - 224] = tw_n(twlo, twhi, ((unsigned)(ht - 224) * (unsigned)(g * kTcCols)) & Nm);
@@ -183,22 +186,25 @@ __device__ __forceinline__ void build_b(float2* __restrict__ tg, int g, int ht, 
         const int off1 = off0 + 256;                                                     // row 8 + j
         const __half2 h0 = __floats2half2_rn(w.x, -w.y);
         const __half2 h1 = __floats2half2_rn(w.y, w.x);
-        const float2 f0 = __half22float2(h0);
-        const float2 f1 = __half22float2(h1);
+        [[maybe_unused]] const float2 f0 = __half22float2(h0);
+        [[maybe_unused]] const float2 f1 = __half22float2(h1);
         *reinterpret_cast<__half2*>(bhi + off0) = h0;
         *reinterpret_cast<__half2*>(bhi + off1) = h1;
-        *reinterpret_cast<__half2*>(blo + off0) = __floats2half2_rn(w.x - f0.x, -w.y - f0.y);
-        *reinterpret_cast<__half2*>(blo + off1) = __floats2half2_rn(w.y - f1.x, w.x - f1.y);
+        if constexpr (LO) {
+            *reinterpret_cast<__half2*>(blo + off0) = __floats2half2_rn(w.x - f0.x, -w.y - f0.y);
+            *reinterpret_cast<__half2*>(blo + off1) = __floats2half2_rn(w.y - f1.x, w.x - f1.y);
+        }
     }
 }
 
-// The MMAs of one group: for each k2 tile, D = A_hi B_hi + A_lo B_hi + A_hi B_lo.
-template <int KP>
+// The MMAs of one group: for each k2 tile, D = A_hi B_hi + A_lo B_hi + A_hi B_lo
+// (LO) or D = A_hi B_hi.
+template <int KP, bool LO = true>
 __device__ __forceinline__ void issue_group(int t, uint32_t tmem, uint32_t dcol, uint32_t bhi, uint32_t blo) {
     {
         const uint32_t d = dcol + 16u * t;
 #pragma unroll
-        for (int p = 0; p < 3; p++) {
+        for (int p = 0; p < (LO ? 3 : 1); p++) {
             const uint32_t a = tmem + (uint32_t)((2 * t + (p == 1 ? 1 : 0)) * KP);
             const uint32_t b = p == 2 ? blo : bhi;
 #pragma unroll
@@ -211,7 +217,8 @@ __device__ __forceinline__ void issue_group(int t, uint32_t tmem, uint32_t dcol,
 // Pre-pass of a row: Z on the window, scaled by 2^e (max |Z| 2^e in
 // [2^14, 2^15)) and split into FP16 hi + lo, into tensor memory as the A
 // operand (tile t, lane 32 q + l holds k2 = l + 32 (8 q + t)). Returns 2^-e.
-template <int KP>
+// Without LO only the hi part is stored.
+template <int KP, bool LO = true>
 __device__ __forceinline__ float tc_prepass(const TcParams& P, const RowDesc& R, const SigDesc& S, uint32_t tmem,
                                             float* s_red) {
     const int tid = threadIdx.x;
@@ -256,15 +263,17 @@ __device__ __forceinline__ float tc_prepass(const TcParams& P, const RowDesc& R,
             const float a = z[ti][k1].x * scale;
             const float b = z[ti][k1].y * scale;
             const __half2 hh = __floats2half2_rn(a, b);
-            const float2 hf = __half22float2(hh);
             hv[k1] = h2bits(hh);
-            lv[k1] = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+            if constexpr (LO) {
+                const float2 hf = __half22float2(hh);
+                lv[k1] = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+            }
         }
         const uint32_t ta = tmem + lane_base + (uint32_t)(2 * t * KP);
 #pragma unroll
         for (int q = 0; q < KP / 8; q++) {
             tmem_st8(ta + 8u * q, hv + 8 * q);
-            tmem_st8(ta + KP + 8u * q, lv + 8 * q);
+            if constexpr (LO) tmem_st8(ta + KP + 8u * q, lv + 8 * q);
         }
     }
     tmem_wait_st();
@@ -450,7 +459,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
 // stage 2, block a1 / 16, row 8 (a1 % 16) + c, so that a warp's stage-2
 // accumulators are [4 a][8 c] tiles of the output staging. Both stages reuse
 // the half's 128 accumulator columns; the phase-1 MMAs of the half's next group
-// are issued once the stage-2 results are in registers.
+// are issued once the stage-2 results are in registers. Phase 1 runs in plain
+// FP16 here (Z and B rounded once, about 2^-12 relative per element), a third
+// of the split-FP16 MMAs: the 16-bit output rounding dominates the error.
 __device__ __forceinline__ void issue_dft_stage(uint32_t d, uint32_t a, uint32_t w) {
 #pragma unroll
     for (int m = 0; m < 2; m++)
@@ -481,7 +492,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const int n = S.n;
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
-    const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
+    const float inv = tc_prepass<KP, false>(P, R, S, tmem, s_red);
     const float s1 = 1.0f / (float)KP;
     const float fin = inv * (float)(KP * 1024);
 
@@ -498,12 +509,12 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        build_b<KP, false>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
             tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group<KP, false>(wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
     }
@@ -516,6 +527,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     // stage-2 accumulators of this thread: a1 = 16 (wl / 4) + 4 qd + lane / 8, column c = lane % 8
     const int my_a1 = 16 * (wl >> 2) + 4 * qd + (lane >> 3);
     const int my_c = lane & 7;
+    unsigned char* my_stage = stage + stage16_off(my_a1, my_c);
     const uint32_t dsrc = dcol + lane_base + 64u * (uint32_t)(wl >> 2);
     if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
     while (g < ng) {
@@ -555,7 +567,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         }
         const int gn = g + 2;
         if (gn < ng) {
-            build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+            build_b<KP, false>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
             fence_proxy_async_smem();
         }
         mbar_wait(mbar2_h, phase2, P.err);
@@ -563,13 +575,14 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         tc_fence_after();
         // stage-1 results of column c = wl, kl = lane: twiddle, stage-2 operand
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            uint32_t r[16];
-            tmem_ld16(dsrc + 16u * q, r);
+        for (int q2 = 0; q2 < 2; q2++) {
+            uint32_t r[32];
+            tmem_ld16(dsrc + 32u * q2, *reinterpret_cast<uint32_t(*)[16]>(r));
+            tmem_ld16(dsrc + 32u * q2 + 16u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
             tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int a1 = 8 * q + i;
+            for (int i = 0; i < 16; i++) {
+                const int a1 = 16 * q2 + i;
                 const float2 v = cmul(make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])),
                                       t2[a1 * 32 + lane]);
                 *reinterpret_cast<uint32_t*>(abuf + (a1 >> 4) * kTcStageBlock + (a1 & 15) * 1024 + a2_off) =
@@ -589,13 +602,14 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         tc_fence_after();
         uint32_t yv[32];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            uint32_t r[16];
-            tmem_ld16(dsrc + 16u * q, r);
+        for (int q2 = 0; q2 < 2; q2++) {
+            uint32_t r[32];
+            tmem_ld16(dsrc + 32u * q2, *reinterpret_cast<uint32_t(*)[16]>(r));
+            tmem_ld16(dsrc + 32u * q2 + 16u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
             tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 8; i++)
-                yv[8 * q + i] = pack16<OT>(
+            for (int i = 0; i < 16; i++)
+                yv[16 * q2 + i] = pack16<OT>(
                     make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
         }
         tc_fence_before();
@@ -603,14 +617,14 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         half_bar(h);  // accumulators free for the next group; staging free
         if (lane == 0 && gn < ng) {
             tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group<KP, false>(wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
+        // a = my_a1 + 32 a2 with my_a1 < 32: box a2 / 8, box row my_a1 + 32 (a2 % 8), same swizzle bit
 #pragma unroll
-        for (int a2 = 0; a2 < 32; a2++) {
-            const int a = my_a1 + 32 * a2;
-            if (a < amax) *reinterpret_cast<unsigned*>(stage + stage16_off(a, my_c)) = yv[a2];
-        }
+        for (int a2 = 0; a2 < 32; a2++)
+            if (my_a1 + 32 * a2 < amax)
+                *reinterpret_cast<unsigned*>(my_stage + (a2 >> 3) * (kBoxBytes / 2) + (a2 & 7) * 1024) = yv[a2];
         const long long row0 = R.out_off + c0;
         constexpr int box_bytes = kBoxBytes / 2;
         if (tma) {
