@@ -1,6 +1,7 @@
 """The two row engines on the same inputs: the tcgen05 tensor-core engine
 (split-FP16 phase-1 GEMM, rows whose window spans <= 16 blocks of 1024 bins,
-N >= 16384) and the CUDA-core engine. Both against the float64 oracle at
+N >= 16384; for 16-bit outputs also the column DFTs, as two radix-32 GEMM
+stages) and the CUDA-core engine. Both against the float64 oracle at
 rel-L2 <= 1e-5 (complex64) and <= 3e-3 (16-bit outputs), and against each
 other. Cases cover the reference's stale bins (sigma 0.5), norm off, complex
 input, odd n, several signals in one plan (plain stores instead of tensor-map
@@ -152,6 +153,41 @@ def test_tensor_engine_device_tensors_repeat(fcwt, oracle, ctx):
     torch.cuda.synchronize()
     p.close()
     assert rel_l2(out.cpu().numpy(), oracle.cwt_fp64(x, sc, 2.0, 1, True)) < TOL
+
+
+@pytest.mark.parametrize("out_type", [1, 2], ids=["bf16", "f16"])
+def test_tensor_engine_16bit_repeat_bit_identical(fcwt, ctx, out_type):
+    """16-bit outputs (column DFTs on the tensor cores) over many rows: every
+    execution gives the same bits (no race between the CTA halves, the
+    staging reuse and the stage MMAs) and matches the complex64 transform of
+    the same plan within the 16-bit tolerance."""
+    import torch
+    from fcwt_b200 import _lib
+
+    ctx.set_engine(_lib.FCWT_ENGINE_TENSOR_CORES)
+    n, fn = 100000, 600
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(n).astype(np.float32)
+    sc = fcwt.Scales(fcwt.Morlet(2.0), fcwt.FCWT_LINFREQS, 1000, 1.0, 101.0, fn)
+    p = fcwt.Plan(n, sc, fb=2.0, threads=1, norm=True)
+    assert p.stats()["tensor_core_rows"] == fn
+    xd = torch.from_numpy(x).cuda()
+    dt = torch.bfloat16 if out_type == 1 else torch.float16
+    outs = []
+    for _ in range(3):
+        o = torch.full((fn, n, 2), float("nan"), dtype=dt, device="cuda")
+        p.execute(xd, o, out_type=out_type)
+        outs.append(o)
+    ref = torch.empty((fn, n), dtype=torch.complex64, device="cuda")
+    p.execute(xd, ref)
+    torch.cuda.synchronize()
+    p.close()
+    for o in outs[1:]:
+        assert torch.equal(o.view(torch.int16), outs[0].view(torch.int16))
+    got = torch.complex(outs[0][..., 0].double(), outs[0][..., 1].double())
+    ref64 = ref.to(torch.complex128)
+    err = float(torch.linalg.vector_norm(got - ref64) / torch.linalg.vector_norm(ref64))
+    assert err < 3e-3
 
 
 def test_tuner_records_engine_choice(fcwt, oracle, ctx, tmp_path, monkeypatch):
