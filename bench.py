@@ -204,7 +204,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-runs", type=int, default=3)
+    ap.add_argument("--cpu-runs", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fn", type=int, default=FN,
                     help="number of rows; values other than 3000 are for profiling captures only")

@@ -101,11 +101,12 @@ def test_tensor_engine_complex_input_odd_n(fcwt, oracle, ctx):
     assert rel_l2(tc, ref) < TOL
 
 
-@pytest.mark.parametrize("n", [100000, 40002], ids=["tensor_map_stores", "plain_stores"])
+@pytest.mark.parametrize("n", [100000, 40002, 16384], ids=["tensor_map_stores", "plain_stores", "smallest_N"])
 @pytest.mark.parametrize("out_type", [1, 2], ids=["bf16", "f16"])
 def test_tensor_engine_16bit_outputs(fcwt, oracle, ctx, out_type, n):
     """16-bit outputs: tensor-map stores when n is a multiple of 4 (16-byte row
-    stride), plain stores otherwise."""
+    stride), plain stores otherwise; N = 16384 is the smallest padded length of
+    the tensor-core engine (16 columns, two groups per row)."""
     from fcwt_b200 import _lib
 
     rng = np.random.default_rng(3)
