@@ -40,10 +40,11 @@ N_SAMPLES = 100_000
 FS = 1000
 F0, F1, FN = 1.0, 101.0, 3000
 SIGMA = 2.0
-# DRAM bytes (read + write) of one k_row_tc launch of this workload: ncu
-# dram__bytes_read.sum 282.39 MB + dram__bytes_write.sum 2.35 GB (one-pass
-# capture of the full-size launch; profiles/k_row_tc_cwt100k_x3000.md)
-TRAFFIC_PER_LAUNCH = 282.39e6 + 2.35e9
+# DRAM bytes (read + write) of one k_row_tc launch of this workload, per
+# output type, from one-pass ncu captures of the full-size launch
+# (dram__bytes_read.sum + dram__bytes_write.sum): complex64
+# profiles/k_row_tc_cwt100k_x3000.md, BF16 profiles/k_row_tc_bf16_cwt100k_x3000.md
+TRAFFIC_PER_LAUNCH = {"complex64": 282.39e6 + 2.35e9, "bf16": 152.88e6 + 1.1459e9}
 
 # --out choices: (constant in fcwt_b200, trailing shape, torch dtype, bytes per point)
 OUT_TYPES = {
@@ -390,7 +391,7 @@ def main():
              "k_row_engine" if st["tensor_core_rows"] == 0 else "k_row_tc + k_row_engine")
     # DRAM bytes of one launch of the row kernel (read + write), from the ncu
     # capture summarised in profiles/ (same workload); per launch like `achieved`
-    traffic = TRAFFIC_PER_LAUNCH if (fn == FN and kname == "k_row_tc" and args.out == "complex64") else None
+    traffic = TRAFFIC_PER_LAUNCH.get(args.out) if (fn == FN and kname == "k_row_tc") else None
     algo = algorithmic_bytes(N_SAMPLES, fn, N, out_bytes)
     achieved = algo / (eng_avg / 1e3) / 1e9
     line = {
