@@ -76,11 +76,23 @@ __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
 }
 
 // ---- bulk-async (TMA) store helpers
+// EVICT_FIRST marks the written lines evict-first in L2 (the output is a
+// stream that is not read again by the kernel).
+template <bool EVICT_FIRST = false>
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* smem, int c0, int c1, int c2) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
-                 ::"l"(reinterpret_cast<unsigned long long>(map)), "r"(s), "r"(c0), "r"(c1), "r"(c2)
-                 : "memory");
+    if constexpr (EVICT_FIRST) {
+        unsigned long long pol;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile(
+            "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%2, %3, %4}], [%1], %5;"
+            ::"l"(reinterpret_cast<unsigned long long>(map)), "r"(s), "r"(c0), "r"(c1), "r"(c2), "l"(pol)
+            : "memory");
+    } else {
+        asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                     ::"l"(reinterpret_cast<unsigned long long>(map)), "r"(s), "r"(c0), "r"(c1), "r"(c2)
+                     : "memory");
+    }
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }

@@ -414,7 +414,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             const int n_full = n / M;
             if (lane == 0 && wl >= 4) {
                 const int j = wl - 4;
-                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
+                // complex64 output lines evict-first in L2 (measured ~1% faster; slower for 4-byte types)
+                if (j * kBoxRows < n_full)
+                    tma_store_3d<OT == OUT_C64>(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
             const int tail = n - n_full * M;
