@@ -44,7 +44,7 @@ SIGMA = 2.0
 # output type, from one-pass ncu captures of the full-size launch
 # (dram__bytes_read.sum + dram__bytes_write.sum): complex64
 # profiles/k_row_tc_cwt100k_x3000.md, BF16 profiles/k_row_tc_bf16_cwt100k_x3000.md
-TRAFFIC_PER_LAUNCH = {"complex64": 282.39e6 + 2.35e9, "bf16": 152.88e6 + 1.1459e9}
+TRAFFIC_PER_LAUNCH = {"complex64": 147.76e6 + 2.3459e9, "bf16": 152.88e6 + 1.1459e9}
 
 # --out choices: (constant in fcwt_b200, trailing shape, torch dtype, bytes per point)
 OUT_TYPES = {
