@@ -465,8 +465,10 @@ __device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0
         __syncthreads();
         const int n_full = n / M;  // stripes a < n_full are complete
         if (tid == 0) {
+            // output lines evict-first in L2: they are not read again, and the
+            // spectrum and scratch the engine re-reads stay resident
             for (int j = 0; j < 4 && j * kBoxRows < n_full; j++)
-                tma_store_3d(omap, stage + j * kBoxBytes, c0, j * kBoxRows, out_row);
+                tma_store_3d<true>(omap, stage + j * kBoxBytes, c0, j * kBoxRows, out_row);
             bulk_commit();
         }
         const int tail = n - n_full * M;  // samples of the partial stripe a = n_full
