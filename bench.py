@@ -42,8 +42,8 @@ F0, F1, FN = 1.0, 101.0, 3000
 SIGMA = 2.0
 # DRAM bytes (read + write) of one k_row_tc launch of this workload, per
 # output type, from one-pass ncu captures of the full-size launch
-# (dram__bytes_read.sum + dram__bytes_write.sum): complex64
-# profiles/k_row_tc_cwt100k_x3000.md, BF16 profiles/k_row_tc_bf16_cwt100k_x3000.md
+# (dram__bytes_read.sum + dram__bytes_write.sum; the capture summaries are
+# kept under profiles/, named for the kernel and the workload)
 TRAFFIC_PER_LAUNCH = {"complex64": 147.76e6 + 2.3459e9, "bf16": 152.88e6 + 1.1459e9}
 
 # --out choices: (constant in fcwt_b200, trailing shape, torch dtype, bytes per point)
