@@ -194,6 +194,12 @@ class Reference:
         L.ref_find2power.restype = ctypes.c_int
         L.ref_cwt_table.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, _vp]
+        L.ref_daughter.argtypes = [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, _vp, _vp, _vp]
+
+    def padded(self, n: int) -> int:
+        """1 << find2power(n) (src/fcwt/fcwt.h:154-165)."""
+        return 1 << self.lib.ref_find2power(int(n))
 
     @staticmethod
     def available(path: str = REF_LIB_PATH) -> bool:
@@ -225,6 +231,34 @@ class Reference:
         self.lib.ref_cwt_table(_ptr(xin), xin.size, 1 if cplx else 0, _ptr(t), t.size, _ptr(sc), sc.size,
                                int(threads), 1 if norm else 0, _ptr(out))
         return out
+
+    def daughter(self, N: int, scales, threads: int, mother=None, inp=None, imaginary: bool = False,
+                 doublesided: bool = False, reset: bool = False) -> np.ndarray:
+        """O1 after FCWT::daughter_wavelet_multiplication of each scale in turn
+        (src/fcwt/fcwt.cpp:197-311), complex64 [fn, N]. Defaults: input all
+        (1 + 0i), mother[w] = w (exact in float32 for N <= 2^24), so a written
+        bin holds its mother-table index. reset: NaN-fill O1 before each row."""
+        sc = np.ascontiguousarray(scales, np.float32)
+        m = np.arange(N, dtype=np.float32) if mother is None else np.ascontiguousarray(mother, np.float32)
+        x = np.ones(N, np.complex64) if inp is None else np.ascontiguousarray(inp, np.complex64)
+        out = np.zeros((sc.size, N), np.complex64)
+        self.lib.ref_daughter(int(N), _ptr(sc), sc.size, int(threads), 1 if imaginary else 0, 1 if doublesided else 0,
+                              1 if reset else 0, _ptr(x), _ptr(m), _ptr(out))
+        return out
+
+    def truncation(self, N: int, scales, threads: int, nidx: int = 64):
+        """The reference's own truncation lengths proc_i (bins its product
+        writes) and mother-table indices idx_i(q) for q < min(nidx, proc_i)
+        (-1 beyond), read back from daughter_wavelet_multiplication."""
+        O = self.daughter(N, scales, threads, reset=True)
+        half = max(N // 2, 1)
+        written = ~np.isnan(O[:, :half].real)
+        proc = np.where(written.all(axis=1), half, np.argmin(written, axis=1)).astype(np.int32)
+        idx = np.full((O.shape[0], nidx), -1, np.int32)
+        for i in range(O.shape[0]):
+            k = min(nidx, int(proc[i]))
+            idx[i, :k] = O[i, :k].real.astype(np.int32)
+        return proc, idx
 
     def support(self, fb: float, scale: float) -> int:
         return self.lib.ref_support(fb, scale)

@@ -16,10 +16,27 @@
 //   ref_cwt_table   -> FCWT::cwt with a Wavelet subclass whose generate(N)
 //                      fills `mother` from a caller table (the reference's
 //                      Wavelet interface, src/fcwt/fcwt.h:67-79)
-#include "fcwt.h"
-
+//   ref_daughter    -> FCWT::daughter_wavelet_multiplication, the per-scale
+//                      product into the reused O1 buffer (src/fcwt/fcwt.cpp:197-311),
+//                      row after row like FCWT::cwt (fcwt.cpp:514-518)
+//
+// daughter_wavelet_multiplication is a private member of FCWT. To call it, the
+// reference header is included with `private` defined as `public` (the
+// standard and FFTW headers it includes are included first, untouched).
+#include <complex>
+#include <cstdlib>
 #include <cstring>
+#include <iostream>
+#include <memory>
 #include <string>
+#include <unistd.h>
+#include <omp.h>
+#include <immintrin.h>
+#include "fftw3.h"
+
+#define private public
+#include "fcwt.h"
+#undef private
 
 extern "C" {
 
@@ -106,6 +123,31 @@ void ref_cwt_table(const void* input, int n, int is_complex, const float* table,
         f.cwt((float*)input, n, (std::complex<float>*)output, &s);
     }
     free(s.scales);
+}
+
+// Runs FCWT(threads)::daughter_wavelet_multiplication for scales[0..fn) in
+// order on one O1 buffer of N bins, with input `in` (N interleaved complex)
+// and table `mother` (N floats), and stores O1 after each row into out[i]
+// (N interleaved complex). reset != 0 fills O1 with NaN before every row (so
+// bins the row does not write stay NaN); reset == 0 starts from zeros and keeps
+// O1 across rows, as FCWT::cwt does.
+void ref_daughter(int N, const float* scales, int fn, int threads, int imaginary, int doublesided, int reset,
+                  const float* in, const float* mother, float* out) {
+    Morlet m(2.0f);
+    FCWT f(&m, threads, false, true);
+    const size_t bytes = sizeof(fftwf_complex) * (size_t)N;
+    fftwf_complex* I = (fftwf_complex*)aligned_alloc(32, (bytes + 31) & ~(size_t)31);
+    fftwf_complex* O = (fftwf_complex*)aligned_alloc(32, (bytes + 31) & ~(size_t)31);
+    std::memcpy(I, in, bytes);
+    std::memset(O, 0, bytes);
+    for (int i = 0; i < fn; i++) {
+        if (reset)
+            for (int q = 0; q < N; q++) O[q][0] = O[q][1] = __builtin_nanf("");
+        f.daughter_wavelet_multiplication(I, O, mother, scales[i], N, imaginary != 0, doublesided != 0);
+        std::memcpy(out + 2 * (size_t)N * (size_t)i, O, bytes);
+    }
+    free(I);
+    free(O);
 }
 
 void ref_create_plan(float fb, int threads, int maxsize, const char* flag) {

@@ -7,7 +7,12 @@ fastlib/fCWT compiled with its shipped FFTW), so they pin both the oracle
 restatement and the GPU path to the reference's behaviour:
   - scale grids and frequencies of the three Scales types;
   - Morlet mother tables (Morlet::generate(int));
-  - per-row truncation lengths (threads 1 and 8) and mother-table indices;
+  - per-row truncation lengths and mother-table indices for threads 1, 8 and
+    16 on every scale case, read back from the reference's own
+    FCWT::daughter_wavelet_multiplication (input 1, mother[w] = w);
+  - per-bin daughter weights as mother-table indices, O1 reused row after
+    row as FCWT::cwt does (stale bins included), for the device test that
+    pushes a delta through a mother[w] = w wavelet;
   - time-domain wavelets (getWavelet);
   - coefficient rows of the reference transform for a 10k x 300 case
     (σ=2, LOGSCALES 1-101 Hz at 1 kHz) and a stale-bin-heavy σ=0.5 case.
@@ -23,7 +28,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from oracle.oracle import LINFREQS, LINSCALES, LOGSCALES, Reference, Restatement  # noqa: E402
+from oracle.oracle import LINFREQS, LINSCALES, LOGSCALES, Reference  # noqa: E402
 
 SCALE_CASES = [
     # (scaletype, fs, f0, f1, fn)
@@ -37,9 +42,14 @@ SCALE_CASES = [
     (LINFREQS, 100, 1.0, 101.0, 300),
 ]
 MOTHER_CASES = [(0.5, 1024), (2.0, 1024), (2.0, 16384), (6.0, 16384), (16.0, 4096)]
-TRUNC_CASES = [
-    # (n, scale case index, threads)
-    (10000, 0, 8), (100000, 1, 1), (100000, 1, 8), (6000, 4, 8), (1001, 3, 1), (2 ** 20, 5, 8), (10000, 7, 3),
+# signal length per scale case (odd lengths included); every case runs with threads 1, 8 and 16
+TRUNC_N = [10000, 100000, 10000, 1001, 6000, 2 ** 20, 123457, 10000]
+TRUNC_CASES = [(TRUNC_N[si], si, T) for si in range(len(SCALE_CASES)) for T in (1, 8, 16)]
+# per-bin weight indices: (n = N, scale case, threads, rows)
+DW_CASES = [
+    (16384, 0, 8, [0, 1, 100, 299]),
+    (32768, 6, 16, [0, 38, 76]),
+    (16384, 4, 1, [0, 150, 299]),
 ]
 
 
@@ -52,7 +62,6 @@ def c1_signal(n=10000, fs=1000, seed=1):
 
 def main():
     ref = Reference()
-    res = Restatement()
     g = {}
     for k, (st, fs, f0, f1, fn) in enumerate(SCALE_CASES):
         g[f"scales_{k}"] = ref.scales(st, fs, f0, f1, fn)
@@ -63,11 +72,18 @@ def main():
     g["mother_cases"] = np.array(MOTHER_CASES, dtype=np.float64)
     for k, (n, si, T) in enumerate(TRUNC_CASES):
         sc = g[f"scales_{si}"]
-        N = res.padded(n)
-        g[f"proc_{k}"] = res.procs(N, sc, T)
+        N = ref.padded(n)
+        proc, idx = ref.truncation(N, sc, T)
+        g[f"proc_{k}"] = proc
         rows = [0, len(sc) // 2, len(sc) - 1]
-        g[f"index_{k}"] = np.stack([res.indices(N, float(sc[r]), 64) for r in rows])
+        g[f"index_{k}"] = idx[rows]
     g["trunc_cases"] = np.array(TRUNC_CASES, dtype=np.int64)
+    for k, (n, si, T, rows) in enumerate(DW_CASES):
+        sc = g[f"scales_{si}"]
+        O = ref.daughter(n, sc, T)  # input 1, mother[w] = w, O1 kept across rows
+        g[f"dw_{k}"] = O[rows, : n // 2].real.astype(np.int32)
+        g[f"dw_rows_{k}"] = np.array(rows, np.int32)
+    g["dw_cases"] = np.array([c[:3] for c in DW_CASES], dtype=np.int64)
     for k, (fb, scale) in enumerate([(2.0, 2.0), (2.0, 10.0), (16.0, 3.5)]):
         pn = 2 * ref.support(fb, scale) + 1
         g[f"wavelet_{k}"] = ref.wavelet(fb, scale, pn)

@@ -210,3 +210,54 @@ def test_large_config_rows_and_linearity(fcwt, oracle):
     got = ox[rows].cpu().numpy()
     assert rel_l2(got, ref) < TOL
     plan.close()
+
+
+class _IndexTable:
+    """A wavelet whose frequency-domain table is mother[w] = w: a row's
+    daughter weight at bin q is then the mother-table index the row uses
+    there (or, for bins past its truncation, the index an earlier row left in
+    the reused O1 buffer)."""
+
+    def __init__(self):
+        self.width = 0
+        self.four_wavelen = 1.0
+        self.imag_frequency = False
+        self.doublesided = False
+        self.mother = None
+
+    def generate(self, size):
+        self.mother = np.arange(size, dtype=np.float32)
+
+
+@pytest.mark.parametrize("mode", ["auto", "cuda_cores"])
+def test_device_weights_equal_reference_daughter_product(fcwt, golden, mode):
+    """The device path's truncation lengths, mother-table indices and reused
+    bins, bit for bit against the reference's own daughter product
+    (src/fcwt/fcwt.cpp:197-311 applied row after row, fcwt.cpp:514-518).
+    A unit impulse has spectrum 1, so row i of the transform (n = N, norm on)
+    is IFFT(W_i) and its float64 FFT returns W_i[q] = idx; rounding recovers
+    the integer index exactly (the float32 transform error is < 0.05 here)."""
+    import torch
+
+    from fcwt_b200 import _lib
+
+    c = _lib.context(0)
+    c.set_engine(_lib.FCWT_ENGINE_AUTO if mode == "auto" else _lib.FCWT_ENGINE_CUDA_CORES)
+    try:
+        for k, (n, si, T) in enumerate(golden["dw_cases"]):
+            n = int(n)
+            sc = golden[f"scales_{si}"]
+            rows = golden[f"dw_rows_{k}"]
+            x = torch.zeros(n, dtype=torch.float32, device="cuda")
+            x[0] = 1.0
+            out = torch.empty((sc.size, n), dtype=torch.complex64, device="cuda")
+            fcwt.FCWT(_IndexTable(), int(T), False, True).cwt(x, sc, out)
+            y = out[torch.from_numpy(rows.astype(np.int64)).cuda()].cpu().numpy().astype(np.complex128)
+            W = np.fft.fft(y, axis=1)
+            half = n // 2
+            err = np.max(np.abs(W[:, :half] - np.round(W[:, :half].real)))
+            assert err < 0.05, (k, err)
+            assert np.max(np.abs(W[:, half:])) < 0.05, k
+            assert np.array_equal(np.round(W[:, :half].real).astype(np.int32), golden[f"dw_{k}"]), (k, mode)
+    finally:
+        c.set_engine(_lib.FCWT_ENGINE_AUTO)

@@ -28,13 +28,44 @@ def test_mother_bit_exact(golden, oracle):
 
 
 def test_truncation_and_indices(golden, oracle):
+    """Truncation lengths and mother-table indices of the restatement equal
+    the ones read back from the reference's own daughter product (every scale
+    case, threads 1, 8 and 16)."""
+    assert {int(T) for _, _, T in golden["trunc_cases"]} == {1, 8, 16}
+    assert len({int(si) for _, si, _ in golden["trunc_cases"]}) == len(golden["scale_cases"])
     for k, (n, si, T) in enumerate(golden["trunc_cases"]):
         sc = golden[f"scales_{si}"]
         N = oracle.padded(int(n))
-        assert np.array_equal(oracle.procs(N, sc, int(T)), golden[f"proc_{k}"]), k
+        proc = golden[f"proc_{k}"]
+        assert np.array_equal(oracle.procs(N, sc, int(T)), proc), k
         rows = [0, len(sc) // 2, len(sc) - 1]
         idx = np.stack([oracle.indices(N, float(sc[r]), 64) for r in rows])
-        assert np.array_equal(idx, golden[f"index_{k}"]), k
+        g = golden[f"index_{k}"]
+        for j, r in enumerate(rows):
+            m = min(64, int(proc[r]))
+            assert np.all(g[j, m:] == -1), (k, r)  # bins the reference does not write
+            assert np.array_equal(idx[j, :m], g[j, :m]), (k, r)
+
+
+def test_daughter_weights_with_reused_bins(golden, oracle):
+    """Per-bin daughter weights of the restatement, including the bins a row
+    inherits from earlier rows through the reused O1 buffer, equal the
+    reference's daughter product row after row (mother[w] = w, so each weight
+    is its mother-table index)."""
+    for k, (n, si, T) in enumerate(golden["dw_cases"]):
+        sc = golden[f"scales_{si}"]
+        rows = golden[f"dw_rows_{k}"]
+        _, W = oracle.weights_rows(int(n), sc, int(T), np.arange(int(n), dtype=np.float32), rows)
+        assert np.array_equal(W[:, : int(n) // 2].astype(np.int32), golden[f"dw_{k}"]), k
+
+
+def test_reference_truncation_reads_back_directly(reference, oracle):
+    """Direct check against the reference build (when present): proc_i for a
+    grid the goldens do not hold."""
+    sc = oracle.scales(LOGSCALES, 44100, 20.0, 20000.0, 200)
+    for T in (1, 4, 32):
+        proc, _ = reference.truncation(65536, sc, T)
+        assert np.array_equal(proc, oracle.procs(65536, sc, T)), T
 
 
 def test_wavelet_time_domain(golden, oracle):
