@@ -33,3 +33,57 @@ def test_traffic_constants_are_per_launch_and_near_algorithmic():
         assert name in bench.OUT_TYPES
         algo = bench.algorithmic_bytes(bench.N_SAMPLES, bench.FN, N, bench.OUT_TYPES[name][3])
         assert 0.9 * algo < traffic < 1.25 * algo
+
+
+def test_both_arms_print_the_same_config():
+    """The reference arm and the GPU arm describe one workload: same keys and
+    values, including the `threads` argument that sets the truncation length."""
+    cfg = bench.plain_config()
+    assert cfg == bench.plain_config(bench.FN, "complex64", bench.THREADS)
+    assert cfg["threads_param"] == bench.THREADS and cfg["fn"] == 3000 and cfg["N"] == 131072
+
+
+def test_reference_arm_loads_no_product_code():
+    """`--impl reference` runs the reference build only: its code path names
+    no fcwt_b200 module."""
+    import inspect
+
+    src = inspect.getsource(bench.run_reference_arm)
+    assert "fcwt_b200" not in src and "_lib" not in src
+
+
+def _shard_worker(rank, world, port, result_path):
+    import os
+
+    import numpy as np
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sh = bench.sharded_transform(compute=lambda x, b, e: None)
+        if rank == 0:
+            np.save(result_path, np.array(sh.blocks))
+        assert sh.rows == sh.blocks[rank]
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_bench_blocks_cover_all_rows(tmp_path):
+    """bench.py --gpus N builds one ShardedCWT over the 100k x 3000 transform:
+    the ranks' contiguous row blocks cover the 3000 rows exactly once."""
+    import socket
+
+    import numpy as np
+    import torch.multiprocessing as mp
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    res = str(tmp_path / "blocks.npy")
+    mp.start_processes(_shard_worker, args=(2, port, res), nprocs=2, join=True, start_method="spawn")
+    blocks = np.load(res)
+    assert blocks[0][0] == 0 and blocks[0][1] == blocks[1][0] and blocks[1][1] == bench.FN
+    assert 0 < blocks[0][1] < bench.FN

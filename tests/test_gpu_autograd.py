@@ -9,27 +9,9 @@ import math
 import numpy as np
 import pytest
 
+from oracle.grad_ref import ref_forward
+
 pytestmark = pytest.mark.gpu
-
-AMP = math.sqrt(2 * math.pi) * 0.75112554446  # the mother table's amplitude
-
-
-def ref_forward(x, sigma, freqs, fs, norm=True):
-    import torch
-
-    B, n = x.shape
-    N = 1 << int(math.ceil(math.log2(n))) if n > 1 else 1
-    X = torch.fft.fft(x, n=N)
-    q = torch.arange(N // 2, dtype=torch.float64, device=x.device)
-    s = fs / freqs
-    u = 2 * math.pi * sigma * (s[:, None] * q[None, :] / N - 1)
-    g = AMP * torch.exp(-0.5 * u * u)
-    Z = torch.zeros((B, freqs.numel(), N), dtype=torch.complex128, device=x.device)
-    Z[..., : N // 2] = X[:, None, : N // 2] * g[None]
-    y = torch.fft.ifft(Z)
-    if not norm:
-        y = y * N
-    return y[..., :n]
 
 
 def loss_fn(y, target):
