@@ -24,6 +24,7 @@ FCWT_NORM = 1 << 0
 FCWT_SCALAR_TRUNC = 1 << 1
 FCWT_EXACT_SUPPORT = 1 << 2
 FCWT_CONTINUOUS = 1 << 3
+FCWT_STRICT = 1 << 4
 
 FCWT_OUT_C64 = 0
 FCWT_OUT_BF16 = 1
@@ -52,6 +53,7 @@ SIGNATURES = {
     "fcwt_profile_read": (_i, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fcwt_find2power": (_i, [_i]),
     "fcwt_scales": (_i, [_i, _i, _f, _f, _i, _vp]),
+    "fcwt_scales_checked": (_i, [_i, _i, _f, _f, _i, _u, _vp]),
     "fcwt_frequencies": (_i, [_vp, _i, _i, _vp]),
     "fcwt_morlet_support": (_i, [_f, _f]),
     "fcwt_morlet_time": (_i, [_f, _f, _i, _vp, _vp]),

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (FCWT_EXACT_SUPPORT, FCWT_NORM, FCWT_OUT_BF16, FCWT_OUT_C64, FCWT_OUT_F16,
-                   FCWT_SCALAR_TRUNC, FcwtError)
+                   FCWT_SCALAR_TRUNC, FCWT_STRICT, FcwtError)
 
 # enum SCALETYPE (src/fcwt/fcwt.h:65)
 FCWT_LINSCALES = 0
@@ -25,6 +25,16 @@ FCWT_LOGSCALES = 1
 FCWT_LINFREQS = 2
 
 _FFTW_FLAGS = {"FFTW_MEASURE": 1, "FFTW_PATIENT": 2, "FFTW_EXHAUSTIVE": 3, "FFTW_ESTIMATE": 0}
+
+
+def _strict(strict) -> bool:
+    """Strict Nyquist checks: the `strict` argument, else FCWT_STRICT=1 in the
+    environment (the reference's asserts, src/fcwt/fcwt.cpp:148,167,184, are
+    compiled out of its release builds, so the default accepts f1 > fs/2)."""
+    if strict is not None:
+        return bool(strict)
+    v = os.environ.get("FCWT_STRICT", "")
+    return bool(v) and v != "0"
 
 
 def _is_torch(x) -> bool:
@@ -155,9 +165,10 @@ class Paul(Wavelet):
         return None
 
 class Scales:
-    """Scales(wavelet, scaletype, fs, f0, f1, fn) (src/fcwt/fcwt.cpp:111-190)."""
+    """Scales(wavelet, scaletype, fs, f0, f1, fn) (src/fcwt/fcwt.cpp:111-190).
+    strict=True (or FCWT_STRICT=1) raises ValueError for f1 > fs/2."""
 
-    def __init__(self, pwav, st, fs, f0, f1, fn):
+    def __init__(self, pwav, st, fs, f0, f1, fn, strict=None):
         fs = _as_int("fs", fs)
         fn = _as_int("fn", fn)
         _positive("f0", f0)
@@ -168,7 +179,12 @@ class Scales:
         self.fourwavl = float(getattr(pwav, "four_wavelen", np.float32(0.9876)))
         self.nscales = fn
         self.scales = np.zeros(fn, np.float32)
-        _lib.call("fcwt_scales", st, fs, ctypes.c_float(f0), ctypes.c_float(f1), fn, _ptr(self.scales))
+        flags = FCWT_STRICT if _strict(strict) else 0
+        rc = _lib.load().fcwt_scales_checked(st, fs, ctypes.c_float(f0), ctypes.c_float(f1), fn, flags,
+                                             _ptr(self.scales))
+        if rc == _lib.FCWT_ERR_INVALID:
+            raise ValueError(_lib.load().fcwt_last_error().decode())
+        _lib.check(rc)
 
     def getScales(self, pfreqs) -> None:
         pfreqs = _inplace_f32(pfreqs)
@@ -200,13 +216,14 @@ class FCWT:
     (src/fcwt/fcwt.h:114-152). ``threads`` keeps its reference meaning for
     the result: it sets the per-scale truncation length (fcwt.cpp:213-214)."""
 
-    def __init__(self, pwav, pthreads, puse_optimalization_schemes, puse_normalization, device: int = 0):
+    def __init__(self, pwav, pthreads, puse_optimalization_schemes, puse_normalization, device: int = 0,
+                 strict=None):
         self.wavelet = pwav
         self.threads = _as_int("pthreads", pthreads)
         self.use_optimalization_schemes = bool(puse_optimalization_schemes)
         self.use_normalization = bool(puse_normalization)
         self.device = device
-        self.flags = FCWT_NORM if self.use_normalization else 0
+        self.flags = (FCWT_NORM if self.use_normalization else 0) | (FCWT_STRICT if _strict(strict) else 0)
 
     # -- tuning files (src/fcwt/fcwt.cpp:313-393)
     def create_FFT_optimization_plan(self, pmaxsize, poptimizationflags) -> None:

@@ -14,6 +14,7 @@
 #include <string>
 #include <array>
 #include <map>
+#include <initializer_list>
 #include <vector>
 
 #include "../../include/fcwt_b200.h"
@@ -98,13 +99,38 @@ struct TuneChoice {
     int engine = 0;       // 0: tensor-core engine for the rows it takes; 1: CUDA-core engine only
 };
 
-bool is_device_pointer(const void* p) {
+// Where a caller's pointer lives: 0 host memory (pageable or pinned), 1 memory
+// the kernels of device `dev` may use directly (that device's memory, or
+// managed memory), -1 another device's memory, which the kernels of `dev`
+// must not touch (without peer access that is an illegal-address fault).
+int pointer_kind(const void* p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
+        return 0;
+    }
+    if (a.type == cudaMemoryTypeManaged) return 1;
+    if (a.type == cudaMemoryTypeDevice) return a.device == dev ? 1 : -1;
+    return 0;
+}
+
+bool is_device_pointer(const void* p) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    return pointer_kind(p, dev) == 1;
+}
+
+// FCWT_OK when no pointer of `ptrs` lives on a device other than `dev`.
+int check_pointer_devices(std::initializer_list<const void*> ptrs, int dev) {
+    for (const void* p : ptrs) {
+        if (p && pointer_kind(p, dev) < 0)
+            return fail(FCWT_ERR_INVALID, "a buffer lives on another GPU than the context's device " +
+                                              std::to_string(dev));
+    }
+    return FCWT_OK;
 }
 
 size_t out_elem_bytes(int out_type) { return out_type == FCWT_OUT_C64 ? 8 : 4; }
@@ -642,6 +668,8 @@ int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs
         const PlanSignal& S = P->sig[(size_t)s];
         if (S.re == S.rb || S.sp.n == 0) continue;
         if (!inputs[s] || !outputs[s]) return fail(FCWT_ERR_INVALID, "null input or output pointer");
+        rc = check_pointer_devices({inputs[s], outputs[s]}, ctx->device);
+        if (rc) return rc;
         in_off[(size_t)s] = in_total;
         if (!is_device_pointer(inputs[s])) in_total += ((size_t)S.sp.n * (S.sp.is_complex ? 8 : 4) + 255) & ~(size_t)255;
         out_off[(size_t)s] = out_total;
@@ -890,6 +918,16 @@ int fcwt_scales(int scaletype, int fs, float f0, float f1, int fn, float* out) {
     return FCWT_OK;
 }
 
+int fcwt_scales_checked(int scaletype, int fs, float f0, float f1, int fn, unsigned flags, float* out) {
+    if (flags & FCWT_STRICT) {
+        if (f1 > (float)fs / 2.0f)
+            return fail(FCWT_ERR_INVALID, "f1 = " + std::to_string(f1) + " Hz is above the Nyquist rate fs/2 = " +
+                                              std::to_string((float)fs / 2.0f) + " Hz");
+        if (scaletype == FCWT_LOGSCALES && !(f0 < f1)) return fail(FCWT_ERR_INVALID, "LOGSCALES needs f0 < f1");
+    }
+    return fcwt_scales(scaletype, fs, f0, f1, fn, out);
+}
+
 int fcwt_frequencies(const float* scales, int fn, int fs, float* out) {
     if (fn < 0 || (fn > 0 && (!out || !scales))) return fail(FCWT_ERR_INVALID, "bad arguments");
     fcwt::host::frequencies(scales, fn, fs, out);
@@ -936,6 +974,8 @@ int fcwt_morlet_mother(fcwt_context* ctx, float fb, int N, float* out) {
     if (rc) return rc;
     if (N <= 0 || !out) return fail(FCWT_ERR_INVALID, "bad arguments");
     if (!(fb > 0.0f)) return fail(FCWT_ERR_INVALID, "bandwidth must be positive");
+    rc = check_pointer_devices({out}, ctx->device);
+    if (rc) return rc;
     if (is_device_pointer(out)) {
         FCWT_CUDA_TRY(fcwt::launch_mother(fb, N, fcwt::host::mother_norm(), out, ctx->stream));
         return FCWT_OK;
@@ -1102,6 +1142,8 @@ int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* co
     const int nsig = (int)plan->sig.size();
     std::vector<const void*> key;
     for (int s = 0; s < nsig; s++) {
+        rc = check_pointer_devices({inputs[s], outputs[s]}, ctx->device);
+        if (rc) return rc;
         if (!is_device_pointer(inputs[s]) || !is_device_pointer(outputs[s]))
             return fail(FCWT_ERR_INVALID, "graph execution needs device inputs and outputs");
         key.push_back(inputs[s]);
@@ -1205,6 +1247,8 @@ int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch
     if (n == 0 || batch == 0) return FCWT_OK;
     if (!x || !grad_out || !grad_x || (fn > 0 && !freqs))
         return fail(FCWT_ERR_INVALID, "null pointer argument");
+    rc = check_pointer_devices({x, grad_out, grad_x}, ctx->device);
+    if (rc) return rc;
     if (!is_device_pointer(x) || !is_device_pointer(grad_out) || !is_device_pointer(grad_x))
         return fail(FCWT_ERR_INVALID, "x, grad_out and grad_x must be device pointers");
     const int log2N = host::find2power(n);

@@ -33,6 +33,13 @@ struct ThreadContext {
 
 thread_local ThreadContext t_ctx;
 
+// FCWT_STRICT=1 in the environment turns on the Nyquist checks the reference
+// makes with (release-disabled) asserts, src/fcwt/fcwt.cpp:148,167,184.
+unsigned strict_flag() {
+    const char* v = std::getenv("FCWT_STRICT");
+    return (v && v[0] && v[0] != '0') ? FCWT_STRICT : 0u;
+}
+
 void check(int rc) {
     if (rc != FCWT_OK) throw std::runtime_error(std::string("fcwt: ") + fcwt_last_error());
 }
@@ -87,7 +94,12 @@ Scales::Scales(Wavelet* wav, SCALETYPE st, int afs, float af0, float af1, int af
     nscales = afn;
     scales = (float*)std::malloc(sizeof(float) * (size_t)(afn > 0 ? afn : 1));
     if (!scales) throw std::bad_alloc();
-    check(fcwt_scales((int)st, afs, af0, af1, afn, scales));
+    const int rc = fcwt_scales_checked((int)st, afs, af0, af1, afn, strict_flag(), scales);
+    if (rc == FCWT_ERR_INVALID) {
+        std::free(scales);
+        throw std::invalid_argument(std::string("fcwt: ") + fcwt_last_error());
+    }
+    check(rc);
 }
 
 Scales::~Scales() { std::free(scales); }
@@ -150,7 +162,7 @@ void FCWT::run(const void* input, bool complexinput, int psize, std::complex<flo
                       << ".wis' was not found, fallback to calculation without optimization." << std::endl;
         }
     }
-    const unsigned flags = use_normalization ? FCWT_NORM : 0u;
+    const unsigned flags = (use_normalization ? FCWT_NORM : 0u) | strict_flag();
     const float* in = reinterpret_cast<const float*>(input);
     if (!m) {
         // any other Wavelet: the table its generate(N) fills, as the reference uses it

@@ -14,6 +14,14 @@
 // queue counters and the scratch ring of the two-phase rows. Its limits:
 // n <= 16384 samples, fn <= 1024 scales, at most 8 distinct stale-bin tables.
 //
+// The call copies nothing from host memory with cudaMemcpy: the row
+// descriptors and stale-bin tables it plans on the host travel to the array
+// as kernel parameters of small copy kernels (each launch carries its own
+// copy of them), and the work list is generated on the device. So no pageable
+// host-to-device copy makes the host wait for earlier work in the stream, and
+// no copy refers to host memory after the call returns. The host-side planning
+// does use the C++ heap; device memory is never allocated.
+//
 // Every call shares that array and leaves its contents behind; each call
 // clears the counters and error word it needs before its kernels run. Calls
 // whose GPU work overlaps (different streams, or different host threads on
@@ -71,6 +79,53 @@ constexpr size_t kNoAllocScratchBytes = align256(kOffScratch + sizeof(float2) * 
 // cudaGetSymbolAddress during the per-device set-up below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// ---- descriptor delivery by kernel parameters (at most 32764 bytes each)
+constexpr int kRowsPerCopy = 232;    // 232 x 104-byte RowDesc
+constexpr int kFloatsPerCopy = 7680; // 30 KB of stale-bin table entries
+
+struct RowCopy {
+    SigDesc sig;
+    int first;
+    int count;
+    int write_sig;
+    int pad;
+    RowDesc rows[kRowsPerCopy];
+};
+struct PoolCopy {
+    int first;
+    int count;
+    float v[kFloatsPerCopy];
+};
+static_assert(sizeof(RowCopy) <= 32000 && sizeof(PoolCopy) <= 32000, "kernel parameter limit");
+
+__global__ void k_na_rows(const __grid_constant__ RowCopy c, RowDesc* __restrict__ dst, SigDesc* __restrict__ dsig) {
+    for (int i = threadIdx.x; i < c.count; i += blockDim.x) dst[c.first + i] = c.rows[i];
+    if (c.write_sig && threadIdx.x == 0) *dsig = c.sig;
+}
+
+__global__ void k_na_pool(const __grid_constant__ PoolCopy c, float* __restrict__ dst) {
+    for (int i = threadIdx.x; i < c.count; i += blockDim.x) dst[c.first + i] = c.v[i];
+}
+
+// The work list of the row engine, the same sequence the host builds for a
+// plan: one item per row when rows run whole (type), otherwise per step s,
+// the n_a phase-1 items of row s (s < fn) followed by the n_b phase-2 items of
+// row s - lag (0 <= s - lag < fn). One thread per step.
+__global__ void k_na_items(int fn, int two_phase, int type, int n_a, int n_b, int lag, Item* __restrict__ items) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!two_phase) {
+        if (s < fn) items[s] = Item{type, s, 0, 0};
+        return;
+    }
+    if (s >= fn + lag) return;
+    int base = n_a * min(s, fn) + n_b * max(0, min(s - lag, fn));
+    if (s < fn)
+        for (int a = 0; a < n_a; a++) items[base++] = Item{ITEM_PHASE1, s, a, 0};
+    const int rb = s - lag;
+    if (rb >= 0 && rb < fn)
+        for (int b = 0; b < n_b; b++) items[base++] = Item{ITEM_PHASE2, rb, b, 0};
+}
+
 int na_fail(int code, const std::string& msg) {
     record_error(msg);
     return code;
@@ -110,13 +165,17 @@ int setup_device(int dev, DeviceSetup** out) {
     return FCWT_OK;
 }
 
-bool on_device(const void* p) {
+// 0 host memory, 1 memory the kernels of device `dev` may use (that device's
+// memory, or managed memory), -1 memory of another device.
+int pointer_kind(const void* p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return 0;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return 1;
+    if (a.type == cudaMemoryTypeDevice) return a.device == dev ? 1 : -1;
+    return 0;
 }
 
 }  // namespace
@@ -139,10 +198,14 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
     if (status) *status = 0;
     if (n == 0 || fn == 0) return FCWT_OK;
     if (!input || !output || !scales) return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: null pointer");
-    if (!on_device(input) || !on_device(output))
-        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: input and output must be device pointers");
     int dev = 0;
     NA_TRY(cudaGetDevice(&dev));
+    if (pointer_kind(input, dev) != 1 || pointer_kind(output, dev) != 1)
+        return na_fail(FCWT_ERR_INVALID,
+                       "fcwt_cwt_noalloc: input and output must be device pointers of the current device " +
+                           std::to_string(dev));
+    if (pointer_kind(scales, dev) != 0)
+        return na_fail(FCWT_ERR_INVALID, "fcwt_cwt_noalloc: scales must be a host array");
     DeviceSetup* S = nullptr;
     int rc = setup_device(dev, &S);
     if (rc) return rc;
@@ -157,14 +220,14 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
     for (const RowPlan& rp : sp.rows)
         if (N >= kP2 && rp.K > kMaxK) return na_fail(FCWT_ERR_UNSUPPORTED, "fcwt_cwt_noalloc: row support too wide");
 
-    // descriptors (same work list as a plan of the row engine)
+    // row descriptors (same rows as a plan of the row engine)
     std::vector<RowDesc> rows((size_t)fn);
-    std::vector<Item> items;
-    std::vector<float> pool;
-    for (const auto& T : sp.tables) pool.insert(pool.end(), T.begin(), T.end());
     const float out_scale = (flags & kFlagNorm) ? 1.0f / (float)N : 1.0f;
     const bool two_phase = N > kMaxFusedN;
-    int S_slots = 0;
+    const int S_slots = two_phase ? std::min(kNaSlots, fn) : 0;
+    const int lag = two_phase ? std::max(1, std::min(12, S_slots / 2)) : 0;
+    const int n_a = two_phase ? kP2 / kChunk : 0;
+    const int n_b = two_phase ? M / kGroupCols : 0;
     for (int r = 0; r < fn; r++) {
         const RowPlan& rp = sp.rows[(size_t)r];
         RowDesc& d = rows[(size_t)r];
@@ -177,8 +240,10 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
         d.lo = rp.lo;
         d.hi = rp.hi;
         d.stale = rp.table >= 0 ? rp.table * sp.half : -1;
-        d.slot = -1;
-        d.wait_row = -1;
+        d.slot = two_phase ? r % S_slots : -1;
+        d.wait_row = two_phase && r >= S_slots ? r - S_slots : -1;
+        d.n_a = n_a;
+        d.n_b = n_b;
         d.out_buf = 0;
         d.out_off = (long long)r * n;
         d.out_scale = out_scale;
@@ -188,28 +253,7 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
         d.cb = rp.cb;
         d.cnorm = host::mother_norm();
     }
-    if (!two_phase) {
-        const int type = N < kP2 ? ITEM_SMALL : ITEM_FUSED;
-        for (int r = 0; r < fn; r++) items.push_back({type, r, 0, 0});
-    } else {
-        S_slots = std::min(kNaSlots, fn);
-        const int D = std::max(1, std::min(12, S_slots / 2));
-        const int n_a = kP2 / kChunk;
-        const int n_b = M / kGroupCols;
-        for (int r = 0; r < fn; r++) {
-            rows[(size_t)r].slot = r % S_slots;
-            rows[(size_t)r].wait_row = r >= S_slots ? r - S_slots : -1;
-            rows[(size_t)r].n_a = n_a;
-            rows[(size_t)r].n_b = n_b;
-        }
-        for (int step = 0; step < fn + D; step++) {
-            if (step < fn)
-                for (int a = 0; a < n_a; a++) items.push_back({ITEM_PHASE1, step, a, 0});
-            const int rb = step - D;
-            if (rb >= 0 && rb < fn)
-                for (int b = 0; b < n_b; b++) items.push_back({ITEM_PHASE2, rb, b, 0});
-        }
-    }
+    const int n_items = two_phase ? fn * (n_a + n_b) : fn;
 
     unsigned char* base = S->base;
     float2* X = reinterpret_cast<float2*>(base + kOffX);
@@ -225,17 +269,40 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
     float2* scratch = reinterpret_cast<float2*>(base + kOffScratch);
 
     cudaStream_t st = (cudaStream_t)stream;
-    SigDesc sd;
-    sd.X = X;
-    sd.mother = mother;
-    sd.tw = tw;
-    sd.log2N = sp.log2N;
-    sd.n = n;
-    NA_TRY(cudaMemcpyAsync(dsig, &sd, sizeof(sd), cudaMemcpyHostToDevice, st));
-    NA_TRY(cudaMemcpyAsync(drows, rows.data(), rows.size() * sizeof(RowDesc), cudaMemcpyHostToDevice, st));
-    NA_TRY(cudaMemcpyAsync(ditems, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice, st));
-    if (!pool.empty())
-        NA_TRY(cudaMemcpyAsync(dpool, pool.data(), pool.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    {
+        // descriptors and stale tables, in kernel-parameter chunks
+        static thread_local RowCopy rc_buf;
+        RowCopy& c = rc_buf;
+        c.sig.X = X;
+        c.sig.mother = mother;
+        c.sig.tw = tw;
+        c.sig.log2N = sp.log2N;
+        c.sig.n = n;
+        for (int r0 = 0; r0 < fn; r0 += kRowsPerCopy) {
+            c.first = r0;
+            c.count = std::min(kRowsPerCopy, fn - r0);
+            c.write_sig = r0 == 0;
+            std::memcpy(c.rows, rows.data() + r0, sizeof(RowDesc) * (size_t)c.count);
+            k_na_rows<<<1, 256, 0, st>>>(c, drows, dsig);
+            NA_TRY(cudaGetLastError());
+        }
+        static thread_local PoolCopy pc_buf;
+        PoolCopy& pc = pc_buf;
+        for (size_t t = 0; t < sp.tables.size(); t++) {
+            const std::vector<float>& T = sp.tables[t];
+            const size_t len = std::min(T.size(), (size_t)sp.half);
+            for (size_t i0 = 0; i0 < len; i0 += kFloatsPerCopy) {
+                pc.first = (int)(t * (size_t)sp.half + i0);  // table t starts at t * half (RowDesc::stale)
+                pc.count = (int)std::min((size_t)kFloatsPerCopy, len - i0);
+                std::memcpy(pc.v, T.data() + i0, sizeof(float) * (size_t)pc.count);
+                k_na_pool<<<1, 256, 0, st>>>(pc, dpool);
+                NA_TRY(cudaGetLastError());
+            }
+        }
+        k_na_items<<<(fn + lag + 127) / 128, 128, 0, st>>>(fn, two_phase ? 1 : 0, N < kP2 ? ITEM_SMALL : ITEM_FUSED,
+                                                             n_a, n_b, lag, ditems);
+        NA_TRY(cudaGetLastError());
+    }
     NA_TRY(cudaMemsetAsync(counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)fn), st));
     NA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), st));
     NA_TRY(launch_mother(fb, N, host::mother_norm(), mother, st));
@@ -247,7 +314,7 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
     ep.sigs = dsig;
     ep.rows = drows;
     ep.items = ditems;
-    ep.n_items = (int)items.size();
+    ep.n_items = n_items;
     ep.stale_pool = dpool;
     ep.scratch = two_phase ? scratch : nullptr;
     ep.slot_elems = two_phase ? N : 0;

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <string>
 
 #include "fcwt_internal.h"
 
@@ -75,6 +76,13 @@ int plan_signal(int n, bool is_complex, float fb, const float* scales, int fn, i
     for (int i = 0; i < fn; i++) {
         if (!(scales[i] > 0.0f) || !std::isfinite(scales[i])) {
             err = "scales must be positive finite numbers";
+            return 1;
+        }
+        // strict mode: centre frequency fs/scale above fs/2 (the reference's
+        // Nyquist asserts, src/fcwt/fcwt.cpp:148,167,184, in terms of the scale)
+        if ((flags & kFlagStrict) && scales[i] < 2.0f) {
+            err = "scale " + std::to_string(scales[i]) + " of row " + std::to_string(i) +
+                  " puts its centre frequency above the Nyquist rate fs/2 (strict mode)";
             return 1;
         }
     }

@@ -12,6 +12,7 @@ constexpr unsigned kFlagNorm = 1u << 0;
 constexpr unsigned kFlagScalarTrunc = 1u << 1;
 constexpr unsigned kFlagExactSupport = 1u << 2;
 constexpr unsigned kFlagContinuous = 1u << 3;
+constexpr unsigned kFlagStrict = 1u << 4;
 
 // Relative weight below which a bin's daughter value is skipped (unless
 // kFlagExactSupport): mother[w] < kTrimRel * max(mother). The skipped terms

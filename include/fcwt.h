@@ -6,20 +6,35 @@
 // unchanged. The transform runs on the GPU through the C ABI in fcwt_b200.h;
 // input and output pointers may be host or device memory.
 //
+// Like the reference header it defines PI, sqrt2PI and IPI4 and brings
+// namespace std into scope (src/fcwt/fcwt.h:59-63), which code written
+// against it relies on (e.g. `complex<float>` unqualified).
+//
 // Differences a caller can observe:
-//   - Only the Morlet wavelet has a GPU transform (the reference ships no
-//     other). A Wavelet that is not a Morlet makes FCWT::cwt throw.
+//   - Any Wavelet subclass works: FCWT::cwt runs on the table its
+//     generate(N) fills, as the reference does (src/fcwt/fcwt.cpp:504-505);
+//     Morlet tables are generated on the GPU.
 //   - Errors (bad sizes, CUDA failures) throw std::runtime_error instead of
-//     being ignored.
+//     being ignored; with FCWT_STRICT=1 in the environment, frequencies above
+//     fs/2 throw std::invalid_argument (the reference's asserts,
+//     src/fcwt/fcwt.cpp:148,167,184, compiled out of its release builds).
 //   - create_FFT_optimization_plan writes tuning files of the GPU engine under
 //     the reference's file names (n<N>_t<threads>.wis).
 #ifndef FCWT_H
 #define FCWT_H
 
 #include <complex>
+#include <iostream>
+#include <memory>
 #include <string>
 
 #define FCWT_LIBRARY_API
+
+#define PI 3.14159265358979323846264338327950288f
+#define sqrt2PI 2.50662827463100050241576528f
+#define IPI4 0.75112554446f
+
+using namespace std;
 
 enum SCALETYPE { FCWT_LINSCALES, FCWT_LOGSCALES, FCWT_LINFREQS };
 

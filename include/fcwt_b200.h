@@ -43,6 +43,10 @@ extern "C" {
 #define FCWT_EXACT_SUPPORT (1u << 2)  /* also evaluate bins whose weight is < 2^-36 of the peak */
 #define FCWT_CONTINUOUS (1u << 3)     /* differentiable Morlet: norm*exp(-(2 pi fb (s q/N - 1))^2/2) at every
                                          bin, no mother-table rounding, truncation or reused bins */
+#define FCWT_STRICT (1u << 4)         /* refuse frequencies above the Nyquist rate fs/2: the reference's
+                                         asserts of src/fcwt/fcwt.cpp:148,167,184, compiled out of its release
+                                         builds. For a transform: any scale < 2 (centre frequency fs/scale >
+                                         fs/2) fails with FCWT_ERR_INVALID */
 
 /* ---- output element types */
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
@@ -95,6 +99,10 @@ int fcwt_profile_read(fcwt_context* ctx, double* engine_ms, int* engine_launches
 int fcwt_find2power(int n);
 /* Scales::Scales(wavelet, st, fs, f0, f1, fn) + getScales, src/fcwt/fcwt.cpp:111-158 */
 int fcwt_scales(int scaletype, int fs, float f0, float f1, int fn, float* scales_out);
+/* The same with flags: FCWT_STRICT makes f1 > fs/2 (any scale type) and, for
+ * LOGSCALES, f0 >= f1 an FCWT_ERR_INVALID (the reference asserts
+ * f1 <= fs/2 in each calculate_*_array, src/fcwt/fcwt.cpp:148,167,184). */
+int fcwt_scales_checked(int scaletype, int fs, float f0, float f1, int fn, unsigned flags, float* scales_out);
 /* Scales::getFrequencies, src/fcwt/fcwt.cpp:133-137 */
 int fcwt_frequencies(const float* scales, int fn, int fs, float* freqs_out);
 /* Morlet::getSupport, src/fcwt/fcwt.h:88 */
@@ -203,13 +211,20 @@ int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const cha
  * allocates nothing: all its device workspace is one static array of about
  * 2.3 MB inside the library (held on every GPU that loads the library).
  * Limits: n <= 16384, fn <= 1024, at most 8 stale-bin tables; larger
- * requests fail with FCWT_ERR_INVALID. input/output must be device pointers;
- * scales is a host array; work is enqueued on `stream` (a cudaStream_t, NULL
- * = legacy default stream). The first call on a device resolves the array's
- * address and configures the kernels for that device: make it before any
- * stream capture. All calls share the array: calls whose GPU work overlaps
+ * requests fail with FCWT_ERR_INVALID. input/output must be device pointers of
+ * the current device; scales is a host array (other pointers fail with
+ * FCWT_ERR_INVALID); work is enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream). The call makes no host-to-device copies: its
+ * descriptors reach the device as kernel parameters, so it does not wait for
+ * earlier work in the stream (host-side planning still uses the C++ heap).
+ * The first call on a device resolves the array's address and configures the
+ * kernels for that device: make it before any stream capture. That address is
+ * kept for the life of the process: do not call cudaDeviceReset while the
+ * library is in use. All calls share the array: calls whose GPU work overlaps
  * race; serialize them on one stream. With status != NULL the call waits for
- * its work and stores the device error word there (0 = ok). */
+ * its work and stores the device error word there (0 = ok); with status ==
+ * NULL it neither waits nor reads that word, so a device-side error is not
+ * reported by this call. */
 int fcwt_cwt_noalloc(const float* input, int n, float fb, const float* scales, int fn, int threads,
                      unsigned flags, void* output, void* stream, int* status);
 

@@ -149,3 +149,33 @@ def test_bin_window_drops_only_negligible_weights(oracle, fcwt, golden, fb, case
             nz = np.nonzero(W[i])[0]
             if nz.size:
                 assert lo_e[i] <= nz[0] and hi_e[i] > nz[-1]
+
+
+def test_strict_nyquist_is_opt_in(fcwt, monkeypatch):
+    """The reference asserts f1 <= fs/2 (src/fcwt/fcwt.cpp:148,167,184) but
+    its release builds compile the asserts out, so by default f1 > fs/2 is
+    accepted (the published benchmark runs fs=100 with f1=101). Strict mode,
+    by argument or FCWT_STRICT=1, refuses it for Scales and for transforms."""
+    monkeypatch.delenv("FCWT_STRICT", raising=False)
+    m = fcwt.Morlet(2.0)
+    s = fcwt.Scales(m, fcwt.FCWT_LINFREQS, 100, 1.0, 101.0, 50)  # accepted, like the release build
+    with pytest.raises(ValueError, match="Nyquist"):
+        fcwt.Scales(m, fcwt.FCWT_LINFREQS, 100, 1.0, 101.0, 50, strict=True)
+    fcwt.Scales(m, fcwt.FCWT_LOGSCALES, 100, 1.0, 50.0, 50, strict=True)  # f1 = fs/2 is fine
+    monkeypatch.setenv("FCWT_STRICT", "1")
+    with pytest.raises(ValueError):
+        fcwt.Scales(m, fcwt.FCWT_LOGSCALES, 1000, 1.0, 600.0, 20)
+    monkeypatch.setenv("FCWT_STRICT", "0")
+    fcwt.Scales(m, fcwt.FCWT_LOGSCALES, 1000, 1.0, 600.0, 20)
+    # transforms: a scale below 2 is a centre frequency above fs/2
+    from fcwt_b200 import _lib
+
+    lib = _lib.load()
+    sc = np.ascontiguousarray(s.scales)
+    proc = np.zeros(sc.size, np.int32)
+    assert sc.min() < 2.0
+    assert lib.fcwt_row_truncation(10000, ctypes.c_float(2.0), sc.ctypes.data, sc.size, 1, 0,
+                                   proc.ctypes.data, None, None) == 0
+    rc = lib.fcwt_row_truncation(10000, ctypes.c_float(2.0), sc.ctypes.data, sc.size, 1, _lib.FCWT_STRICT,
+                                 proc.ctypes.data, None, None)
+    assert rc == _lib.FCWT_ERR_INVALID and b"Nyquist" in lib.fcwt_last_error()

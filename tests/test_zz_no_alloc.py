@@ -78,3 +78,23 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
     rc, _ = _noalloc(lib, torch.zeros(100, device="cuda"), sc2, 2.0, 1, True, out2)
     assert rc == _lib.FCWT_ERR_INVALID
     assert b"1024" in lib.fcwt_last_error()
+
+
+def test_noalloc_rejects_a_device_scales_array():
+    """scales is read on the host: a device pointer is refused with an error,
+    not dereferenced."""
+    import torch
+
+    from fcwt_b200 import _lib
+
+    lib = _lib.load()
+    n, fn = 1000, 4
+    x = torch.zeros(n, device="cuda")
+    out = torch.empty((fn, n), dtype=torch.complex64, device="cuda")
+    sc_dev = torch.full((fn,), 10.0, device="cuda")
+    status = ctypes.c_int(-1)
+    rc = lib.fcwt_cwt_noalloc(ctypes.c_void_p(x.data_ptr()), n, ctypes.c_float(2.0),
+                              ctypes.c_void_p(sc_dev.data_ptr()), fn, 1, 1, ctypes.c_void_p(out.data_ptr()),
+                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), ctypes.byref(status))
+    assert rc == _lib.FCWT_ERR_INVALID
+    assert b"host" in lib.fcwt_last_error()
