@@ -8,10 +8,10 @@ of lib/libfcwt_b200.so; there is no CPU fallback.
 """
 from ._lib import (FcwtError, FCWT_OUT_BF16, FCWT_OUT_C64, FCWT_OUT_DB, FCWT_OUT_F16,  # noqa: F401
                    FCWT_OUT_POWER, LIB_PATH)
-from .api import (FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, BatchPlan, Morlet, Paul, Plan,  # noqa: F401
+from .api import (DOG, FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, BatchPlan, Morlet, Paul, Plan,  # noqa: F401
                   Scales, Wavelet, cwt, cwt_device, mother_host, row_truncation, synchronize)
 
-__all__ = ["Morlet", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
+__all__ = ["Morlet", "Paul", "DOG", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
            "cwt_device", "Plan", "BatchPlan", "synchronize", "row_truncation", "mother_host", "FcwtError",
            "morlet_cwt", "LearnableMorletCWT"]
 

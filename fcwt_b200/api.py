@@ -164,6 +164,49 @@ class Paul(Wavelet):
         self.mother = t.astype(np.float32)
         return None
 
+class DOG(Wavelet):
+    """Derivative-of-Gaussian wavelet of order m (real in time, so its
+    spectrum is two-sided: doublesided; odd orders are imaginary in
+    frequency: imag_frequency). The reference names DOG(order) in its test
+    suite and main.cpp (tests/test_fcwt.py:156-182, src/main.cpp:68, both
+    commented out) but defines no class; this one follows the published
+    spectrum psi^(w) = -i^m / sqrt(Gamma(m + 1/2)) w^m exp(-w^2/2) (Torrence &
+    Compo 1998), stretched like Paul so the peak of |psi^| sits where the
+    Morlet's does (table entry w = N/2, so Scales maps scale s to fs / s):
+
+        mother[w] = A * s_m * y^m * exp(m (1 - y^2) / 2),   y = 2 w / N,
+
+    A the Morlet table's peak value and s_m the sign of -i^m once the factor
+    i of odd orders is left to imag_frequency (s_m = -1, 1, 1, -1 for
+    m = 1, 2, 3, 4, period 4). The transform runs through the caller-wavelet
+    path with FCWT_DOUBLESIDED (and FCWT_IMAG_FREQUENCY for odd m), the
+    reference's own semantics for those flags (src/fcwt/fcwt.cpp:232-273)."""
+
+    def __init__(self, order: int = 2):
+        super().__init__()
+        self.m = int(order)
+        if self.m < 1:
+            raise ValueError("order must be >= 1")
+        self.four_wavelen = 1.0
+        self.imag_frequency = self.m % 2 == 1
+        self.doublesided = True
+
+    def generate(self, *args):
+        if len(args) != 1:
+            raise NotImplementedError("DOG provides the frequency-domain table generate(size) only")
+        size = _as_int("size", args[0])
+        w = np.arange(max(size, 0), dtype=np.float64)
+        y = 2.0 * w / max(size, 1)
+        amp = np.sqrt(2.0 * np.pi) * 0.75112554446
+        sign = -1.0 if (self.m % 4) in (0, 1) else 1.0
+        with np.errstate(under="ignore"):
+            t = sign * amp * np.exp(self.m * np.log(np.maximum(y, 1e-300)) + 0.5 * self.m * (1.0 - y * y))
+        t[y == 0] = 0.0
+        self.width = size
+        self.mother = t.astype(np.float32)
+        return None
+
+
 class Scales:
     """Scales(wavelet, scaletype, fs, f0, f1, fn) (src/fcwt/fcwt.cpp:111-190).
     strict=True (or FCWT_STRICT=1) raises ValueError for f1 > fs/2."""
@@ -274,8 +317,8 @@ class FCWT:
             ctx.set_stream(torch.cuda.current_stream(out.device).cuda_stream)
             try:
                 _lib.call("fcwt_cwt_mother", ctx.handle, ctypes.c_void_p(x.data_ptr()), n, 1 if complex_input else 0,
-                          _ptr(table), table.size, _ptr(sc), sc.size, self.threads, self.flags,
-                          ctypes.c_void_p(out.data_ptr()), out_type)
+                          _ptr(table), table.size, _ptr(sc), sc.size, self.threads,
+                          self.flags | _kind_flags(self.wavelet), ctypes.c_void_p(out.data_ptr()), out_type)
             finally:
                 ctx.set_stream(None)
             return
@@ -284,7 +327,7 @@ class FCWT:
         table = _table_of(self.wavelet, n)
         _check_host_output(out, sc.size, n, out_type)
         _lib.call("fcwt_cwt_mother", ctx.handle, _ptr(xin), n, 1 if complex_input else 0, _ptr(table), table.size,
-                  _ptr(sc), sc.size, self.threads, self.flags, _ptr(out), out_type)
+                  _ptr(sc), sc.size, self.threads, self.flags | _kind_flags(self.wavelet), _ptr(out), out_type)
 
     def _run(self, x, scales, out, complex_input: bool, out_type: int) -> None:
         sc = _scales_array(scales)
@@ -305,11 +348,20 @@ class FCWT:
                   self.flags, _ptr(out), out_type)
 
 
+def _kind_flags(wavelet) -> int:
+    """FCWT_IMAG_FREQUENCY / FCWT_DOUBLESIDED from the wavelet's fields (the
+    reference passes them to its product, src/fcwt/fcwt.cpp:396-429)."""
+    f = 0
+    if getattr(wavelet, "imag_frequency", False):
+        f |= _lib.FCWT_IMAG_FREQUENCY
+    if getattr(wavelet, "doublesided", False):
+        f |= _lib.FCWT_DOUBLESIDED
+    return f
+
+
 def _table_of(wavelet, n: int) -> np.ndarray:
     """The frequency-domain table wavelet.generate(N) fills, N = 2^find2power(n)
     (the reference reads wavelet->mother after generate, fcwt.cpp:504-505)."""
-    if getattr(wavelet, "imag_frequency", False) or getattr(wavelet, "doublesided", False):
-        raise NotImplementedError("wavelets with imag_frequency or doublesided are not supported")
     N = 1 << _lib.load().fcwt_find2power(int(n))
     wavelet.generate(N)
     t = getattr(wavelet, "mother", None)

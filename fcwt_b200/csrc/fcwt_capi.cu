@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -45,6 +46,9 @@ cudaError_t tc_configure();
 cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const int* row_list, int n_list,
                               const float* pool, float* wts, cudaStream_t st);
 cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st);
+cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStream_t st);
+cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int log2N,
+                                       const float2* tw, float sgn, cudaStream_t st);
 }  // namespace fcwt
 
 namespace {
@@ -131,6 +135,13 @@ int check_pointer_devices(std::initializer_list<const void*> ptrs, int dev) {
                                               std::to_string(dev));
     }
     return FCWT_OK;
+}
+
+// Kernel variant switch read from the environment (0/1), `def` when unset.
+int tc_variant(const char* name, int def) {
+    const char* v = std::getenv(name);
+    if (!v || !v[0]) return def;
+    return v[0] != '0' ? 1 : 0;
 }
 
 size_t out_elem_bytes(int out_type) { return out_type == FCWT_OUT_C64 ? 8 : 4; }
@@ -247,6 +258,9 @@ struct fcwt_plan {
     int n_rows = 0;
     int n_tc = 0;  // rows run by the tensor-core engine
     std::vector<float> custom_mother;  // caller's wavelet table (N floats), empty for Morlet(fb)
+    bool imag = false;         // wavelet with imag_frequency: every product times i
+    bool doublesided = false;  // wavelet with doublesided: second pass on the shifted spectrum
+    DevBuf Xs, sigs2, ds_tmp;  // doublesided: shifted spectrum, its signal descriptor, second-pass rows
     int slots = 0;
     long long slot_elems = 0;
     bool two_phase = false;
@@ -281,6 +295,9 @@ void plan_free(fcwt_plan* p) {
     p->graph_jobs.release();
     p->tc_rows.release();
     p->tc_wts.release();
+    p->Xs.release();
+    p->sigs2.release();
+    p->ds_tmp.release();
     if (p->jobs_host) cudaFreeHost(p->jobs_host);
     delete p;
 }
@@ -347,6 +364,7 @@ int plan_build(fcwt_plan* P) {
             d.cb = rp.cb;
             d.cnorm = host::mother_norm();
             d.kp = 0;
+            d.imag = P->imag ? 1 : 0;
             const int g = (int)rows.size();
             // tensor-core rows: window [L, L + 1024 kp), L a multiple of 1024, kp <= 16
             int tc_kp = 0;
@@ -488,6 +506,15 @@ int plan_build(fcwt_plan* P) {
         FCWT_CUDA_TRY(cudaStreamSynchronize(st));
         owners.release();
     }
+    if (P->doublesided) {
+        const PlanSignal& S = P->sig[0];
+        FCWT_CUDA_TRY(P->Xs.ensure((size_t)S.sp.N * sizeof(float2)));
+        SigDesc s2 = sds[0];
+        s2.X = P->Xs.as<float2>();
+        FCWT_CUDA_TRY(P->sigs2.ensure(sizeof(SigDesc)));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->sigs2.p, &s2, sizeof(SigDesc), cudaMemcpyHostToDevice, st));
+        FCWT_CUDA_TRY(P->ds_tmp.ensure(std::max<size_t>((size_t)(S.re - S.rb) * (size_t)S.sp.n, 1) * sizeof(float2)));
+    }
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;
 }
@@ -533,6 +560,8 @@ void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int,
     job_groups(P, groups);
 }
 
+int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type);
+
 // Enqueues the forward FFTs and the row engine for device-resident inputs and
 // outputs (no host synchronisation, so it can be captured into a graph).
 // graph_jobs: device copy of the forward jobs prepared before a capture.
@@ -542,6 +571,8 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     fcwt_context* ctx = P->ctx;
     cudaStream_t st = ctx->stream;
     const int nsig = (int)P->sig.size();
+    if (P->doublesided && out_type != FCWT_OUT_C64)
+        return fail(FCWT_ERR_UNSUPPORTED, "doublesided wavelets write complex64 outputs only");
     if (nsig == 1) {
         PlanSignal& S = P->sig[0];
         FCWT_CUDA_TRY(ctx->tmp.ensure((size_t)S.sp.N * sizeof(float2)));
@@ -572,16 +603,57 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
             off += g.second;
         }
     }
+    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    const bool prof = ctx->profiling && allow_profiling;
+    if (prof) {
+        if (!ctx->ev_free.empty()) {
+            ev = ctx->ev_free.back();
+            ctx->ev_free.pop_back();
+        } else {
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
+        }
+        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
+    }
+    int rc = enqueue_rows(P, P->sigs.as<SigDesc>(), dout, out_type);
+    if (rc) return rc;
+    if (P->doublesided) {
+        // the mirrored half: exp(-2 pi i t / N) conj(V), V the rows on the shifted spectrum
+        const PlanSignal& S = P->sig[0];
+        const float2* tw = P->tables[(size_t)S.table].tw.as<float2>();
+        FCWT_CUDA_TRY(launch_shift_spectrum(S.X.as<float2>(), S.sp.log2N, P->Xs.as<float2>(), st));
+        void* tmp_out[1] = {P->ds_tmp.p};
+        rc = enqueue_rows(P, P->sigs2.as<SigDesc>(), tmp_out, out_type);
+        if (rc) return rc;
+        FCWT_CUDA_TRY(launch_doublesided_combine(static_cast<float2*>(dout[0]), P->ds_tmp.as<float2>(),
+                                                 S.re - S.rb, S.sp.n, S.sp.log2N, tw, P->imag ? -1.0f : 1.0f, st));
+        ctx->kernel_launches += 2;
+    }
+    if (prof) {
+        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
+        ctx->ev_used.push_back(ev);
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return FCWT_OK;
+}
+
+// The row-engine launches of one pass over the plan's rows, reading the
+// spectra of `dsigs` and writing `dout`.
+int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    cudaStream_t st = ctx->stream;
+    const int nsig = (int)P->sig.size();
     const size_t n_counters = plan_counters(P);
     FCWT_CUDA_TRY(ctx->counters.ensure(n_counters * sizeof(unsigned)));
     FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, n_counters * sizeof(unsigned), st));
-    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
-    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
     if (P->two_phase)
         FCWT_CUDA_TRY(ctx->scratch.ensure((size_t)P->slots * (size_t)P->slot_elems * sizeof(float2)));
     EngineParams ep;
     std::memset(&ep, 0, sizeof(ep));
-    ep.sigs = P->sigs.as<SigDesc>();
+    ep.sigs = dsigs;
     ep.rows = P->rows.as<RowDesc>();
     ep.items = P->items.as<Item>();
     ep.n_items = P->n_items;
@@ -606,18 +678,6 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     // the CUDA-core engine stages complex64 boxes only
     ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64) ? map_ok : 0;
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
-    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
-    const bool prof = ctx->profiling && allow_profiling;
-    if (prof) {
-        if (!ctx->ev_free.empty()) {
-            ev = ctx->ev_free.back();
-            ctx->ev_free.pop_back();
-        } else {
-            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
-            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
-        }
-        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
-    }
     if (P->n_tc > 0) {
         TcParams tp;
         std::memset(&tp, 0, sizeof(tp));
@@ -631,6 +691,8 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         for (int s = 0; s < nsig; s++) tp.outs[s] = dout[s];
         tp.err = ep.err;
         tp.tma_store = map_ok;
+        tp.c64_dft = tc_variant("FCWT_TC_C64_DFT", 0);
+        tp.direct16 = tc_variant("FCWT_TC_DIRECT16", 0);
         FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_tc, ctx->num_sms)), st));
         ctx->kernel_launches += 1;
     }
@@ -638,11 +700,6 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         FCWT_CUDA_TRY(launch_engine(ep, omap, grid, st));
         ctx->kernel_launches += 1;
     }
-    if (prof) {
-        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
-        ctx->ev_used.push_back(ev);
-    }
-    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     return FCWT_OK;
 }
 
@@ -1044,11 +1101,14 @@ int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const floa
                                           " values");
     for (int i = 0; i < N; i++)
         if (!std::isfinite(mother[i])) return fail(FCWT_ERR_INVALID, "the mother table holds a non-finite value");
+    if ((flags & FCWT_DOUBLESIDED) && N < 2) return fail(FCWT_ERR_INVALID, "doublesided wavelets need n >= 2");
     fcwt_plan* P = new fcwt_plan();
     P->ctx = ctx;
     P->fb = 1.0f;
     P->is_complex = is_complex != 0;
     P->custom_mother.assign(mother, mother + N);
+    P->imag = (flags & FCWT_IMAG_FREQUENCY) != 0;
+    P->doublesided = (flags & FCWT_DOUBLESIDED) != 0;
     P->sig.resize(1);
     P->sig[0].rb = row_begin;
     P->sig[0].re = row_end;

@@ -165,15 +165,15 @@ void FCWT::run(const void* input, bool complexinput, int psize, std::complex<flo
     const unsigned flags = (use_normalization ? FCWT_NORM : 0u) | strict_flag();
     const float* in = reinterpret_cast<const float*>(input);
     if (!m) {
-        // any other Wavelet: the table its generate(N) fills, as the reference uses it
-        // (src/fcwt/fcwt.cpp:504-505); single-sided real wavelets only
-        if (wavelet->imag_frequency || wavelet->doublesided)
-            throw std::runtime_error("fcwt: wavelets with imag_frequency or doublesided are not supported");
+        // any other Wavelet: the table its generate(N) fills and its imag_frequency /
+        // doublesided fields, as the reference uses them (src/fcwt/fcwt.cpp:396-429, 504-505)
         const int N = 1 << find2power(psize);
         wavelet->generate(N);
         if (!wavelet->mother) throw std::runtime_error("fcwt: Wavelet::generate(N) left mother empty");
+        const unsigned kind = (wavelet->imag_frequency ? FCWT_IMAG_FREQUENCY : 0u) |
+                              (wavelet->doublesided ? FCWT_DOUBLESIDED : 0u);
         check(fcwt_cwt_mother(ctx, input, psize, complexinput ? 1 : 0, wavelet->mother, N, scales->scales,
-                              scales->nscales, threads, flags, poutput, FCWT_OUT_C64));
+                              scales->nscales, threads, flags | kind, poutput, FCWT_OUT_C64));
         check(fcwt_synchronize(ctx));
         return;
     }

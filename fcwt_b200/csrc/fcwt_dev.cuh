@@ -56,7 +56,8 @@ __device__ __forceinline__ float2 bin_value(const RowDesc& R, const SigDesc& S, 
     if (q < R.lo || q >= R.hi) return make_float2(0.0f, 0.0f);
     const float m = bin_weight(R, S.mother, pool, nm1, q) * R.out_scale;
     const float2 xv = __ldg(S.X + q);
-    return make_float2(xv.x * m, xv.y * m);
+    // imag_frequency: i * m * Ihat (the reference's AVX product, src/fcwt/fcwt.cpp:255-262)
+    return R.imag ? make_float2(-xv.y * m, xv.x * m) : make_float2(xv.x * m, xv.y * m);
 }
 
 template <int OT>

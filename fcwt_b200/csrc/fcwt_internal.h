@@ -66,6 +66,8 @@ struct RowDesc {
     float cnorm;      // continuous Morlet amplitude (the mother table's norm)
     int kp;           // tensor-core rows: 1024-bin blocks of the window, padded to 8 or 16
     long long woff;   // tensor-core rows: offset of the row's 1024*kp weights in the plan's table
+    int imag;         // 1: wavelet with imag_frequency, every product multiplied by i
+    int pad_;
 };
 
 enum ItemType : int { ITEM_FUSED = 0, ITEM_PHASE1 = 1, ITEM_PHASE2 = 2, ITEM_SMALL = 3, ITEM_PHASE1W = 4 };
@@ -127,6 +129,8 @@ struct TcParams {
     void* outs[kMaxOuts];
     int* err;
     int tma_store;             // outputs via the tensor map (buffer 0, complex64, even n)
+    int c64_dft;               // complex64 rows: column DFTs as split-FP16 tensor-core stages
+    int direct16;              // 16-bit outputs: stores straight from the stage-2 results (no staging)
 };
 
 // Error bits written by device code into EngineParams::err.

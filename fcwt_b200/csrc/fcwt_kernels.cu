@@ -679,6 +679,59 @@ cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st) {
 
 // Forward FFT of the zero-padded input into `out` (N complex values), using
 // `tmp` (N complex) as the ping-pong buffer.
+// ---- doublesided wavelets (src/fcwt/fcwt.cpp:241-273): the product also
+// writes bins b in [N - proc, N) with weight mother[idx(N - 1 - b)] on the
+// mirrored spectrum Ihat[b] = conj(Ihat[N - b]) (fcwt.cpp:507-510). With
+// q = N - 1 - b that half of a row is exp(-2 pi i t / N) conj(V[t]), V the
+// ordinary single-sided row of the same weights on the shifted spectrum
+//     J[q] = Ihat[q + 1] (q < N/2 - 1),  J[N/2 - 1] = conj(Ihat[N/2]).
+namespace dev {
+__global__ void k_shift_spectrum(const float2* __restrict__ X, int N, float2* __restrict__ J) {
+    const int half = N >> 1;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < N; q += gridDim.x * blockDim.x) {
+        float2 v = make_float2(0.0f, 0.0f);
+        if (q + 1 < half)
+            v = X[q + 1];
+        else if (q + 1 == half)
+            v = make_float2(X[half].x, -X[half].y);
+        J[q] = v;
+    }
+}
+
+// out[r][t] += sgn * exp(-2 pi i t / N) * conj(V[r][t]) for rows r < rows, t < n.
+__global__ void k_doublesided_combine(float2* __restrict__ out, const float2* __restrict__ V, long long rows, int n,
+                                      int log2N, const float2* __restrict__ tw, float sgn) {
+    const long long total = rows * (long long)n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(i % n);
+        const float2 w = tw_lookup(tw, log2N, (unsigned)t);  // exp(+2 pi i t / N)
+        const float2 v = V[i];
+        // exp(-2 pi i t/N) conj(v) = conj(w v)
+        const float2 p = cmul(w, v);
+        float2 o = out[i];
+        o.x += sgn * p.x;
+        o.y -= sgn * p.y;
+        out[i] = o;
+    }
+}
+}  // namespace dev
+
+cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStream_t st) {
+    const int N = 1 << log2N;
+    dev::k_shift_spectrum<<<std::max(1, std::min(1184, (N + 255) / 256)), 256, 0, st>>>(X, N, J);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int log2N,
+                                       const float2* tw, float sgn, cudaStream_t st) {
+    const long long total = rows * (long long)n;
+    if (total <= 0) return cudaSuccess;
+    const int grid = (int)std::max(1LL, std::min(148LL * 16, (total + 255) / 256));
+    dev::k_doublesided_combine<<<grid, 256, 0, st>>>(out, V, rows, n, log2N, tw, sgn);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
                            float2* out, float2* tmp, cudaStream_t st, int* n_kernels) {
     const int N = 1 << log2N;

@@ -47,6 +47,13 @@ extern "C" {
                                          asserts of src/fcwt/fcwt.cpp:148,167,184, compiled out of its release
                                          builds. For a transform: any scale < 2 (centre frequency fs/scale >
                                          fs/2) fails with FCWT_ERR_INVALID */
+/* Wavelet kinds of the reference's Wavelet interface (fields imag_frequency and
+ * doublesided, src/fcwt/fcwt.h:75), for caller tables (fcwt_plan_create_mother
+ * / fcwt_cwt_mother), with the semantics of the reference's shipped (AVX)
+ * product, src/fcwt/fcwt.cpp:232-273: */
+#define FCWT_IMAG_FREQUENCY (1u << 5) /* every product is i * mother[idx] * Ihat[q] */
+#define FCWT_DOUBLESIDED (1u << 6)    /* bins b in [N - proc, N) are also written, with weight
+                                         mother[idx(N - 1 - b)] on the mirrored spectrum (complex64 output) */
 
 /* ---- output element types */
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */
@@ -147,9 +154,12 @@ int fcwt_plan_destroy(fcwt_plan* plan);
 /* A caller-supplied wavelet: the reference's FCWT::cwt takes any Wavelet*
  * and uses the table its generate(N) fills (src/fcwt/fcwt.cpp:504-505,
  * fcwt.h:67-79). `mother` (host memory) holds that table, N =
- * 2^find2power(n) floats; single-sided real wavelets (imag_frequency and
- * doublesided false, the only kind the reference defines). Truncation,
- * indices and reused bins follow the reference exactly as for Morlet. */
+ * 2^find2power(n) floats. Truncation,
+ * indices and reused bins follow the reference exactly as for Morlet.
+ * FCWT_IMAG_FREQUENCY / FCWT_DOUBLESIDED in `flags` select the other wavelet
+ * kinds of the reference's product (a doublesided row is computed as two
+ * single-sided passes, the second on the spectrum shifted by one bin, and a
+ * combine; complex64 output only). */
 int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const float* mother, int mother_size,
                             const float* scales, int fn, int threads, unsigned flags, int row_begin, int row_end,
                             fcwt_plan** plan);

@@ -145,13 +145,18 @@ class Restatement:
         return sel, W
 
     def cwt_fp64(self, x, scales, fb: float, threads: int = 1, norm: bool = True,
-                 avx: bool = True, rows=None, mother=None) -> np.ndarray:
+                 avx: bool = True, rows=None, mother=None, imaginary: bool = False,
+                 doublesided: bool = False) -> np.ndarray:
         """Float64 restatement of FCWT::cwt (src/fcwt/fcwt.cpp:447-529) with the
         reference's exact truncation, indices and stale-bin weights, and
         float64 FFTs. `mother` replaces the Morlet(fb) table by a caller's
         frequency-domain table of N entries (the Wavelet::generate(N) result,
-        fcwt.cpp:504-505). Returns complex128 [fn, n], or [len(rows), n] for
-        the selected rows (ascending)."""
+        fcwt.cpp:504-505). imaginary / doublesided: the wavelet's
+        imag_frequency / doublesided fields with the AVX product's semantics
+        (fcwt.cpp:232-273): products times i; bins b in [N - proc, N) of the
+        mirrored spectrum (fcwt.cpp:507-510) weighted by the row's weight at
+        N - 1 - b (reused bins included). Returns complex128 [fn, n], or
+        [len(rows), n] for the selected rows (ascending)."""
         x = np.asarray(x)
         n = x.size
         N = self.padded(n)
@@ -164,9 +169,18 @@ class Restatement:
         _, W = self.weights_rows(N, scales, threads, table, sel, avx)
         half = N // 2
         out = np.zeros((len(sel), n), np.complex128)
+        if doublesided and N > 1:
+            Im = Ihat.copy()
+            i = np.arange(1, half)
+            Im[N - i] = np.conj(Ihat[i])
         for k in range(len(sel)):
             O1 = np.zeros(N, np.complex128)
             O1[:half] = Ihat[:half] * W[k, :half].astype(np.float64)
+            if doublesided and N > 1:
+                b = np.arange(half, N)
+                O1[half:] = Im[half:] * W[k, N - 1 - b].astype(np.float64)
+            if imaginary:
+                O1 *= 1j
             y = np.fft.ifft(O1)  # includes the 1/N
             if not norm:
                 y = y * N
@@ -193,7 +207,7 @@ class Reference:
                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]
         L.ref_find2power.restype = ctypes.c_int
         L.ref_cwt_table.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int,
-                                    ctypes.c_int, ctypes.c_int, _vp]
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]
         L.ref_daughter.argtypes = [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, _vp, _vp, _vp]
 
@@ -220,16 +234,19 @@ class Reference:
         self.lib.ref_mother(fb, N, _ptr(out))
         return out
 
-    def cwt_table(self, x, table, scales, threads: int = 1, norm: bool = True) -> np.ndarray:
-        """FCWT::cwt with a wavelet whose generate(N) returns `table`."""
+    def cwt_table(self, x, table, scales, threads: int = 1, norm: bool = True, imaginary: bool = False,
+                  doublesided: bool = False) -> np.ndarray:
+        """FCWT::cwt with a wavelet whose generate(N) returns `table` and whose
+        imag_frequency / doublesided fields are set as given."""
         x = np.asarray(x)
         cplx = np.iscomplexobj(x)
         xin = np.ascontiguousarray(x, np.complex64 if cplx else np.float32)
         sc = np.ascontiguousarray(scales, np.float32)
         t = np.ascontiguousarray(table, np.float32)
         out = np.zeros((sc.size, xin.size), np.complex64)
+        kind = (1 if imaginary else 0) | (2 if doublesided else 0)
         self.lib.ref_cwt_table(_ptr(xin), xin.size, 1 if cplx else 0, _ptr(t), t.size, _ptr(sc), sc.size,
-                               int(threads), 1 if norm else 0, _ptr(out))
+                               int(threads), 1 if norm else 0, kind, _ptr(out))
         return out
 
     def daughter(self, N: int, scales, threads: int, mother=None, inp=None, imaginary: bool = False,

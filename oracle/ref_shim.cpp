@@ -93,9 +93,9 @@ void ref_cwt(const void* input, int n, int is_complex, float fb, const float* sc
 // user subclass of the reference's Wavelet would provide it.
 class TableWavelet : public Wavelet {
 public:
-    TableWavelet(const float* t, int n) : table(t), size(n) {
-        imag_frequency = false;
-        doublesided = false;
+    TableWavelet(const float* t, int n, int kind) : table(t), size(n) {
+        imag_frequency = (kind & 1) != 0;
+        doublesided = (kind & 2) != 0;
         four_wavelen = 1.0f;
         mother = nullptr;
     }
@@ -110,9 +110,11 @@ public:
     int size;
 };
 
+// kind: bit 0 imag_frequency, bit 1 doublesided (the Wavelet fields the
+// reference's product reads, src/fcwt/fcwt.cpp:396-429)
 void ref_cwt_table(const void* input, int n, int is_complex, const float* table, int table_size,
-                   const float* scales, int fn, int threads, int norm, void* output) {
-    TableWavelet w(table, table_size);
+                   const float* scales, int fn, int threads, int norm, int kind, void* output) {
+    TableWavelet w(table, table_size, kind);
     Morlet m(2.0f);
     Scales s(&m, FCWT_LOGSCALES, 1000, 1.0f, 2.0f, fn);
     std::memcpy(s.scales, scales, sizeof(float) * (size_t)fn);
