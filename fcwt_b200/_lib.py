@@ -67,6 +67,8 @@ SIGNATURES = {
     "fcwt_ccwt": (_i, [_vp, _vp, _i, _f, _vp, _i, _i, _u, _vp, _i]),
     "fcwt_plan_create": (_i, [_vp, _i, _i, _f, _vp, _i, _i, _u, _i, _i, ctypes.POINTER(_vp)]),
     "fcwt_plan_execute": (_i, [_vp, _vp, _vp, _i]),
+    "fcwt_plan_create_strided": (_i, [_vp, _i, _i, _f, _vp, _i, _i, _u, _i, _i, _i, _i, ctypes.POINTER(_vp)]),
+    "fcwt_plan_output_shape": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fcwt_plan_destroy": (_i, [_vp]),
     "fcwt_plan_stats": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fcwt_plan_create_mother": (_i, [_vp, _i, _i, _vp, _i, _vp, _i, _i, _u, _i, _i, ctypes.POINTER(_vp)]),

@@ -434,11 +434,15 @@ class Plan:
     flag-dependent work done once; ``execute`` runs one transform.
 
     rows=(begin, end) selects a shard of the scale rows (multi-GPU sharding);
-    the reference's stale-bin semantics still follow all rows."""
+    the reference's stale-bin semantics still follow all rows.
+    row_stride / time_stride: fused decimation (fcwt_plan_create_strided):
+    every row_stride-th row of the shard and every time_stride-th sample
+    (a power of two), output [ceil(rows / row_stride), ceil(n / time_stride)]."""
 
     def __init__(self, n: int, scales, fb: float = 2.0, threads: int = 1, norm: bool = True,
                  complex_input: bool = False, rows: tuple[int, int] | None = None, device: int = 0,
-                 exact_support: bool = False, scalar_trunc: bool = False):
+                 exact_support: bool = False, scalar_trunc: bool = False, row_stride: int = 1,
+                 time_stride: int = 1):
         self.ctx = _lib.context(device)
         self.device = device
         self.scales = _scales_array(scales).copy()
@@ -449,14 +453,22 @@ class Plan:
         flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0) | \
             (FCWT_SCALAR_TRUNC if scalar_trunc else 0)
         h = ctypes.c_void_p()
-        _lib.call("fcwt_plan_create", self.ctx.handle, self.n, 1 if complex_input else 0, ctypes.c_float(fb),
-                  _ptr(self.scales), self.fn, int(threads), flags, int(self.rows[0]), int(self.rows[1]),
-                  ctypes.byref(h))
+        if row_stride == 1 and time_stride == 1:
+            _lib.call("fcwt_plan_create", self.ctx.handle, self.n, 1 if complex_input else 0, ctypes.c_float(fb),
+                      _ptr(self.scales), self.fn, int(threads), flags, int(self.rows[0]), int(self.rows[1]),
+                      ctypes.byref(h))
+        else:
+            _lib.call("fcwt_plan_create_strided", self.ctx.handle, self.n, 1 if complex_input else 0,
+                      ctypes.c_float(fb), _ptr(self.scales), self.fn, int(threads), flags, int(self.rows[0]),
+                      int(self.rows[1]), int(row_stride), int(time_stride), ctypes.byref(h))
         self.handle = h
+        r, c = ctypes.c_int(), ctypes.c_int()
+        _lib.call("fcwt_plan_output_shape", self.handle, ctypes.byref(r), ctypes.byref(c))
+        self.out_shape = (r.value, c.value)
 
     @property
     def n_rows(self) -> int:
-        return self.rows[1] - self.rows[0]
+        return self.out_shape[0]
 
     def execute(self, x, out, out_type: int = FCWT_OUT_C64, stream=None) -> None:
         """x, out: numpy arrays (host; synchronous) or torch CUDA tensors (enqueued
@@ -475,7 +487,7 @@ class Plan:
         xin = _host_input(x, self.complex_input)
         if xin.size != self.n:
             raise ValueError("input length differs from the plan")
-        _check_host_output(out, self.n_rows, self.n, out_type)
+        _check_host_output(out, self.out_shape[0], self.out_shape[1], out_type)
         _lib.call("fcwt_plan_execute", self.handle, _ptr(xin), _ptr(out), out_type)
 
     def stats(self) -> dict:

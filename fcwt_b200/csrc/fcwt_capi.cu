@@ -47,7 +47,7 @@ cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const in
                               const float* pool, float* wts, cudaStream_t st);
 cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st);
 cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStream_t st);
-cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int log2N,
+cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int dec, int log2N,
                                        const float2* tw, float sgn, cudaStream_t st);
 }  // namespace fcwt
 
@@ -234,7 +234,11 @@ struct fcwt_context {
 // One signal of a plan.
 struct PlanSignal {
     fcwt::SignalPlan sp;
-    int rb = 0, re = 0;  // rows of this signal produced by the plan
+    int rb = 0, re = 0;  // rows of this signal produced by the plan: rb, rb + rstride, ... < re
+    int rstride = 1;     // row decimation
+    int dec = 1;         // time decimation (power of two): output sample t' is y[dec t']
+    int rows_out() const { return re > rb ? (re - rb + rstride - 1) / rstride : 0; }
+    int n_out() const { return (sp.n + dec - 1) / dec; }
     int row0 = 0;        // global index of its first produced row
     int table = 0;       // index into fcwt_plan::tables
     DevBuf X;            // forward spectrum, N complex
@@ -341,8 +345,14 @@ int plan_build(fcwt_plan* P) {
         if ((long long)pool.size() > (1ll << 30)) return fail(FCWT_ERR_INVALID, "stale-bin tables too large");
         const float out_scale = (sp.flags & kFlagNorm) ? 1.0f / (float)sp.N : 1.0f;
         S.row0 = (int)rows.size();
-        for (int r = S.rb; r < S.re; r++) {
+        const int Mfull = sp.N >= kP2 ? sp.N / kP2 : 1;
+        if (S.dec > 1 && sp.N > kMaxFusedN && Mfull / S.dec < kGroupCols)
+            return fail(FCWT_ERR_UNSUPPORTED, "time decimation " + std::to_string(S.dec) + " needs N >= 8192 x " +
+                                                  std::to_string(S.dec) + " for a padded length above 8192 (N = " +
+                                                  std::to_string(sp.N) + ")");
+        for (int r = S.rb; r < S.re; r += S.rstride) {
             const RowPlan& rp = sp.rows[(size_t)r];
+            const int ro = (r - S.rb) / S.rstride;  // output row
             RowDesc d;
             std::memset(&d, 0, sizeof(d));
             d.sig = s;
@@ -356,9 +366,11 @@ int plan_build(fcwt_plan* P) {
             d.slot = -1;
             d.wait_row = -1;
             d.out_buf = s;
-            d.out_off = (long long)(r - S.rb) * sp.n;
+            d.dec = S.dec;
+            d.n_out = S.n_out();
+            d.out_off = (long long)ro * d.n_out;
             d.out_scale = out_scale;
-            d.out_row = r - S.rb;
+            d.out_row = ro;
             d.mode = (sp.flags & kFlagContinuous) ? 1 : 0;
             d.ca = rp.ca;
             d.cb = rp.cb;
@@ -370,7 +382,7 @@ int plan_build(fcwt_plan* P) {
             int tc_kp = 0;
             const bool tc_on = ctx->engine_mode == FCWT_ENGINE_TENSOR_CORES ||
                                (ctx->engine_mode == FCWT_ENGINE_AUTO && ctx->tune[sp.log2N].engine == 0);
-            if (tc_on && sp.N >= kTcMinN) {
+            if (tc_on && sp.N >= kTcMinN && Mfull / S.dec >= kGroupCols) {
                 const int L = rp.hi > rp.lo ? (rp.lo / kP2) * kP2 : 0;
                 const int kw = rp.hi > rp.lo ? (rp.hi - L + kP2 - 1) / kP2 : 0;
                 if (kw <= kTcMaxKp) tc_kp = kw <= 8 ? 8 : 16;
@@ -431,7 +443,7 @@ int plan_build(fcwt_plan* P) {
             d.slot = i % S;
             d.wait_row = i >= S ? two_phase_rows[(size_t)(i - S)] : -1;
             d.n_a = d.K > kMaxK ? kP2 / kWideChunk : kP2 / kChunk;
-            d.n_b = M / kGroupCols;
+            d.n_b = M / d.dec / kGroupCols;
         }
         for (int step = 0; step < nt + D; step++) {
             if (step < nt) {
@@ -513,7 +525,7 @@ int plan_build(fcwt_plan* P) {
         s2.X = P->Xs.as<float2>();
         FCWT_CUDA_TRY(P->sigs2.ensure(sizeof(SigDesc)));
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->sigs2.p, &s2, sizeof(SigDesc), cudaMemcpyHostToDevice, st));
-        FCWT_CUDA_TRY(P->ds_tmp.ensure(std::max<size_t>((size_t)(S.re - S.rb) * (size_t)S.sp.n, 1) * sizeof(float2)));
+        FCWT_CUDA_TRY(P->ds_tmp.ensure(std::max<size_t>((size_t)S.rows_out() * (size_t)S.n_out(), 1) * sizeof(float2)));
     }
     FCWT_CUDA_TRY(cudaStreamSynchronize(st));
     return FCWT_OK;
@@ -628,7 +640,8 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         rc = enqueue_rows(P, P->sigs2.as<SigDesc>(), tmp_out, out_type);
         if (rc) return rc;
         FCWT_CUDA_TRY(launch_doublesided_combine(static_cast<float2*>(dout[0]), P->ds_tmp.as<float2>(),
-                                                 S.re - S.rb, S.sp.n, S.sp.log2N, tw, P->imag ? -1.0f : 1.0f, st));
+                                                 S.rows_out(), S.n_out(), S.dec, S.sp.log2N, tw,
+                                                 P->imag ? -1.0f : 1.0f, st));
         ctx->kernel_launches += 2;
     }
     if (prof) {
@@ -671,9 +684,9 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
     if (nsig == 1 && (P->two_phase || P->n_tc > 0)) {
         const PlanSignal& S = P->sig[0];
         if (out_type == FCWT_OUT_C64)
-            map_ok = encode_output_map(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
+            map_ok = encode_output_map(dout[0], S.n_out(), S.sp.M / S.dec, S.rows_out(), &omap) ? 1 : 0;
         else
-            map_ok = encode_output_map16(dout[0], S.sp.n, S.sp.M, S.re - S.rb, &omap) ? 1 : 0;
+            map_ok = encode_output_map16(dout[0], S.n_out(), S.sp.M / S.dec, S.rows_out(), &omap) ? 1 : 0;
     }
     // the CUDA-core engine stages complex64 boxes only
     ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64) ? map_ok : 0;
@@ -730,7 +743,7 @@ int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs
         in_off[(size_t)s] = in_total;
         if (!is_device_pointer(inputs[s])) in_total += ((size_t)S.sp.n * (S.sp.is_complex ? 8 : 4) + 255) & ~(size_t)255;
         out_off[(size_t)s] = out_total;
-        out_bytes[(size_t)s] = (size_t)(S.re - S.rb) * (size_t)S.sp.n * out_elem_bytes(out_type);
+        out_bytes[(size_t)s] = (size_t)S.rows_out() * (size_t)S.n_out() * out_elem_bytes(out_type);
         if (!is_device_pointer(outputs[s])) out_total += (out_bytes[(size_t)s] + 255) & ~(size_t)255;
     }
     if (in_total) FCWT_CUDA_TRY(ctx->in_stage.ensure(in_total));
@@ -1078,6 +1091,57 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
         return rc;
     }
     *out = P;
+    return FCWT_OK;
+}
+
+int fcwt_plan_create_strided(fcwt_context* ctx, int n, int is_complex, float fb, const float* scales, int fn,
+                             int threads, unsigned flags, int row_begin, int row_end, int row_stride,
+                             int time_stride, fcwt_plan** out) {
+    int rc = ctx_prepare(ctx);
+    if (rc) return rc;
+    if (!out) return fail(FCWT_ERR_INVALID, "null plan output");
+    *out = nullptr;
+    if (row_stride < 1) return fail(FCWT_ERR_INVALID, "row_stride must be >= 1");
+    if (time_stride < 1 || (time_stride & (time_stride - 1)))
+        return fail(FCWT_ERR_INVALID, "time_stride must be a power of two >= 1");
+    if (fn < 0 || n < 0) return fail(FCWT_ERR_INVALID, "negative size");
+    if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
+    if (row_begin < 0 || row_end > fn || row_begin > row_end)
+        return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
+    fcwt_plan* P = new fcwt_plan();
+    P->ctx = ctx;
+    P->fb = fb;
+    P->is_complex = is_complex != 0;
+    P->sig.resize(1);
+    P->sig[0].rb = row_begin;
+    P->sig[0].re = row_end;
+    P->sig[0].rstride = row_stride;
+    P->sig[0].dec = time_stride;
+    std::string err;
+    if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sig[0].sp, err)) {
+        delete P;
+        return fail(FCWT_ERR_INVALID, err);
+    }
+    if (time_stride > std::max(1, n)) {
+        delete P;
+        return fail(FCWT_ERR_INVALID, "time_stride larger than the signal");
+    }
+    rc = plan_build(P);
+    if (rc) {
+        std::string keep = g_err;
+        plan_free(P);
+        g_err = keep;
+        return rc;
+    }
+    *out = P;
+    return FCWT_OK;
+}
+
+int fcwt_plan_output_shape(const fcwt_plan* plan, int* rows, int* cols) {
+    if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (plan->sig.size() != 1) return fail(FCWT_ERR_INVALID, "batched plans have one shape per signal");
+    if (rows) *rows = plan->sig[0].rows_out();
+    if (cols) *cols = plan->sig[0].n_out();
     return FCWT_OK;
 }
 

@@ -67,6 +67,8 @@ struct RowDesc {
     int kp;           // tensor-core rows: 1024-bin blocks of the window, padded to 8 or 16
     long long woff;   // tensor-core rows: offset of the row's 1024*kp weights in the plan's table
     int imag;         // 1: wavelet with imag_frequency, every product multiplied by i
+    int dec;          // time decimation D (power of two): output sample t' is y[D t']
+    int n_out;        // output samples of the row: ceil(n / D)
     int pad_;
 };
 

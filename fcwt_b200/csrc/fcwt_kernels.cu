@@ -442,14 +442,18 @@ __device__ __forceinline__ void dft1024_warp(float2 (&x)[32], int lane, float2* 
 // thread 0 and completed asynchronously; the partial last stripe a = n / M is
 // stored by threads) or, without a tensor map, as runs of 8 samples stored by
 // all threads from a padded SMEM tile.
+//
+// Time decimation D: output sample t' = c' + M a (M = the decimated column
+// count N / 1024 / D, n = the decimated length) is y[D t'], i.e. column
+// c = D c' of G; only those columns are transformed.
 template <int OT>
-__device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0, int M, int n, void* outb,
+__device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0, int M, int n, int D, void* outb,
                                          long long out_off, int out_row, float2* __restrict__ region0,
                                          const float2* __restrict__ t2, const CUtensorMap* omap, bool tma) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const float2* __restrict__ col = G + (size_t)(c0 + warp) * kP2 + lane;
+    const float2* __restrict__ col = G + (size_t)(c0 + warp) * (size_t)D * kP2 + lane;
     float2 x[32];
 #pragma unroll
     for (int m = 0; m < 32; m++) x[m] = __ldcg(col + 32 * m);
@@ -571,7 +575,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             const float nm1 = (float)N - 1.0f;
             for (int q = lo + tid; q < hi; q += kThreads) zs[q - lo] = bin_value(R, S, P.stale_pool, nm1, q);
             __syncthreads();
-            for (int t = tid; t < n; t += kThreads) {
+            for (int to = tid; to < R.n_out; to += kThreads) {
+                const int t = to * R.dec;
                 float2 acc = make_float2(0.0f, 0.0f);
                 for (int q = lo; q < hi; q++) {
                     const float2 w = twlo[(q * t) & (N - 1)];
@@ -579,7 +584,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     acc.x += z.x * w.x - z.y * w.y;
                     acc.y += z.x * w.y + z.y * w.x;
                 }
-                store_out<OT>(outb, R.out_off + t, acc);
+                store_out<OT>(outb, R.out_off + to, acc);
             }
         } else if (item.type == ITEM_FUSED) {
             // whole row in this CTA (N <= 8192, M <= 8 columns): phase 1 into
@@ -601,10 +606,11 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             __syncthreads();
             const int log2M = log2N - kLog2P2;
-            for (int t = tid; t < n; t += kThreads) {
+            for (int to = tid; to < R.n_out; to += kThreads) {
+                const int t = to * R.dec;
                 const int c = t & (M - 1);
                 const int a = t >> log2M;
-                store_out<OT>(outb, R.out_off + t, region0[a * kStagePitch + c]);
+                store_out<OT>(outb, R.out_off + to, region0[a * kStagePitch + c]);
             }
         } else if (item.type == ITEM_PHASE1) {
             if (tid == 0) {
@@ -641,8 +647,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             __syncthreads();
             if (s_ok) {
                 const float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
-                phase2_item<OT>(G, item.part * kGroupCols, N >> kLog2P2, n, outb, R.out_off, R.out_row, region0, t2,
-                                &omap, P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0);
+                phase2_item<OT>(G, item.part * kGroupCols, (N >> kLog2P2) / R.dec, R.n_out, R.dec, outb, R.out_off,
+                                R.out_row, region0, t2, &omap, P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(b_done + item.row, 1u);
@@ -698,13 +704,14 @@ __global__ void k_shift_spectrum(const float2* __restrict__ X, int N, float2* __
     }
 }
 
-// out[r][t] += sgn * exp(-2 pi i t / N) * conj(V[r][t]) for rows r < rows, t < n.
+// out[r][t'] += sgn * exp(-2 pi i t / N) * conj(V[r][t']) for rows r < rows,
+// output samples t' < n (t = dec t', the row's sample).
 __global__ void k_doublesided_combine(float2* __restrict__ out, const float2* __restrict__ V, long long rows, int n,
-                                      int log2N, const float2* __restrict__ tw, float sgn) {
+                                      int dec, int log2N, const float2* __restrict__ tw, float sgn) {
     const long long total = rows * (long long)n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int t = (int)(i % n);
+        const int t = (int)(i % n) * dec;
         const float2 w = tw_lookup(tw, log2N, (unsigned)t);  // exp(+2 pi i t / N)
         const float2 v = V[i];
         // exp(-2 pi i t/N) conj(v) = conj(w v)
@@ -723,12 +730,12 @@ cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStr
     return cudaGetLastError();
 }
 
-cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int log2N,
+cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int dec, int log2N,
                                        const float2* tw, float sgn, cudaStream_t st) {
     const long long total = rows * (long long)n;
     if (total <= 0) return cudaSuccess;
     const int grid = (int)std::max(1LL, std::min(148LL * 16, (total + 255) / 256));
-    dev::k_doublesided_combine<<<grid, 256, 0, st>>>(out, V, rows, n, log2N, tw, sgn);
+    dev::k_doublesided_combine<<<grid, 256, 0, st>>>(out, V, rows, n, dec, log2N, tw, sgn);
     return cudaGetLastError();
 }
 

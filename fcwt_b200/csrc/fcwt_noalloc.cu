@@ -245,6 +245,8 @@ extern "C" int fcwt_cwt_noalloc(const float* input, int n, float fb, const float
         d.n_a = n_a;
         d.n_b = n_b;
         d.out_buf = 0;
+        d.dec = 1;
+        d.n_out = n;
         d.out_off = (long long)r * n;
         d.out_scale = out_scale;
         d.out_row = r;

@@ -172,14 +172,16 @@ __device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, floa
 // K index 2 k1 + {re, im}; byte offset of element (n, k) in the canonical
 // K-major layout: (k / 16) * 512 + (n / 8) * 256 + ((k / 8) % 2) * 128 +
 // (n % 8) * 16 + (k % 8) * 2.
+// With time decimation D the group's columns are c = D (8 g + j).
 template <int KP, bool LO = true>
 __device__ __forceinline__ void build_b(float2* __restrict__ tg, int g, int ht, int M, unsigned Nm, int L, const float2* __restrict__ twlo,
-                                        const float2* __restrict__ twhi, unsigned char* bhi, unsigned char* blo) {
-    if (ht >= 224) tg[ht - 224] = tw_n(twlo, twhi, ((unsigned)(ht - 224) * (unsigned)(g * kTcCols)) & Nm);
+                                        const float2* __restrict__ twhi, unsigned char* bhi, unsigned char* blo,
+                                        int D = 1) {
+    if (ht >= 224) tg[ht - 224] = tw_n(twlo, twhi, ((unsigned)(ht - 224) * (unsigned)(D * g * kTcCols)) & Nm);
     if (ht < kTcCols * KP) {
         const int j = ht / KP;
         const int k1 = ht - j * KP;
-        const int c = g * kTcCols + j;
+        const int c = D * (g * kTcCols + j);
         const float2 w = cmul(twhi[(unsigned)(k1 * c) & (unsigned)(M - 1)],
                               tw_n(twlo, twhi, ((unsigned)L * (unsigned)c) & Nm));
         const int k = 2 * k1;
@@ -319,13 +321,15 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int N = 1 << log2N;
     const int M = N >> kLog2P2;
     const unsigned Nm = (unsigned)N - 1u;
-    const int n = S.n;
+    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
+    const int Mo = M / D;
+    const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
     const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
 
     // ---- column groups
-    const int ng = M / kTcCols;
+    const int ng = Mo / kTcCols;
     float2* gbuf = reinterpret_cast<float2*>(sm + h * kTcGbufBytes);
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
     unsigned char* blo = bhi + kTcBBytes;
@@ -336,7 +340,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
@@ -346,7 +350,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         }
     }
     const int tb = (wl >> 2) * 4;  // this warp drains tiles tb .. tb + 3
-    const int amax = (n + M - 1) / M;  // stripes a that hold output samples
+    const int amax = (n + Mo - 1) / Mo;  // stripes a that hold output samples
     // the halves run the same per-group sequence; starting half 1 a little later
     // keeps their DFT (issue-bound) and staging/store (SMEM-bound) phases apart
     if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
@@ -354,7 +358,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
         tc_fence_after();
-        const int c0 = g * kTcCols;
+        const int c0 = g * kTcCols;  // first output column c' of the group (column D c0 of the row)
         float2 gv[4][kTcCols];
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
@@ -362,8 +366,8 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
             tmem_wait_ld();
             const int k2 = lane + 32 * (8 * qd + tb + tt);
-            float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], inv));
-            const float2 stp = twlo[k2];
+            float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], inv));
+            const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
 #pragma unroll
             for (int j = 0; j < kTcCols; j++) {
                 gv[tt][j] = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
@@ -374,7 +378,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators drained; the G buffer is free
         const int gn = g + 2;
-        if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
             const int k2 = lane + 32 * (8 * qd + tb + tt);
@@ -412,7 +416,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (tma) {
             fence_proxy_async_smem();
             half_bar(h);
-            const int n_full = n / M;
+            const int n_full = n / Mo;
             if (lane == 0 && wl >= 4) {
                 const int j = wl - 4;
                 // complex64 output lines evict-first in L2 (measured ~1% faster; slower for 4-byte types)
@@ -420,9 +424,9 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
                     tma_store_3d<OT == OUT_C64>(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
-            const int tail = n - n_full * M;
+            const int tail = n - n_full * Mo;
             if (ht < kTcCols && c0 + ht < tail && n_full < kP2) {
-                const long long idx = row0 + ht + (long long)M * n_full;
+                const long long idx = row0 + ht + (long long)Mo * n_full;
                 if constexpr (OT == OUT_C64)
                     store_out<OT>(outb, idx, *reinterpret_cast<const float2*>(stage + stage_off(n_full, ht)));
                 else
@@ -434,8 +438,8 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             for (int idx = ht; idx < kTcCols * kP2; idx += 256) {
                 const int w = idx & (kTcCols - 1);
                 const int a = idx >> 3;
-                if (c0 + w + (long long)M * a < n) {
-                    const long long o = row0 + w + (long long)M * a;
+                if (c0 + w + (long long)Mo * a < n) {
+                    const long long o = row0 + w + (long long)Mo * a;
                     if constexpr (OT == OUT_C64)
                         store_out<OT>(outb, o, *reinterpret_cast<const float2*>(stage + stage_off(a, w)));
                     else
@@ -525,14 +529,16 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
     const int N = 1 << log2N;
     const int M = N >> kLog2P2;
     const unsigned Nm = (unsigned)N - 1u;
-    const int n = S.n;
+    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
+    const int Mo = M / D;
+    const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
     const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
     const float s1 = 1.0f / (float)KP;
     const float fin = inv * (float)(KP * 1024);
 
-    const int ng = M / kTcCols;
+    const int ng = Mo / kTcCols;
     unsigned char* ahi = sm + h * kTcGbufBytes;  // stage operand, high parts (32 KB)
     unsigned char* alo = ahi + kTcGbufBytes / 2; // stage operand, low parts (32 KB)
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
@@ -545,7 +551,7 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
     float2* outb = reinterpret_cast<float2*>(P.outs[R.out_buf]);
     int g = h;
     if (g < ng) {
-        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
@@ -555,7 +561,7 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
         }
     }
     const int tb = (wl >> 2) * 4;
-    const int amax = (n + M - 1) / M;
+    const int amax = (n + Mo - 1) / Mo;
     const uint32_t a1_off = (uint32_t)((lane >> 3) * 1024 + (lane & 7) * 128 + ((((2 * qd + (tb >> 2)) ^ lane) & 7) << 4));
     const uint32_t a2_off = (uint32_t)(wl * 128 + ((((lane >> 2) ^ wl) & 7) << 4) + (lane & 3) * 4);
     const int my_a1 = 16 * (wl >> 2) + 4 * qd + (lane >> 3);
@@ -566,7 +572,7 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
         tc_fence_after();
-        const int c0 = g * kTcCols;
+        const int c0 = g * kTcCols;  // first output column c' of the group (column D c0 of the row)
         // two tiles at a time: each thread's 16-byte piece of a row holds kb = 8 qd + tb + 0..3,
         // written as two 8-byte halves (tt = 0, 1 and tt = 2, 3)
 #pragma unroll
@@ -579,8 +585,8 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
                 tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
                 tmem_wait_ld();
                 const int k2 = lane + 32 * (8 * qd + tb + tt);
-                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], s1));
-                const float2 stp = twlo[k2];
+                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], s1));
+                const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
 #pragma unroll
                 for (int j = 0; j < kTcCols; j++) {
                     split_h2(cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w), ph[j][u],
@@ -605,7 +611,7 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
         }
         const int gn = g + 2;
         if (gn < ng) {
-            build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+            build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
             fence_proxy_async_smem();
         }
         mbar_wait(mbar2_h, phase2, P.err);
@@ -651,8 +657,8 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const int a = my_a1 + 32 * i;
-            if (a < amax && c + (long long)M * a < n)
-                __stcs(orow + (long long)M * a,
+            if (a < amax && c + (long long)Mo * a < n)
+                __stcs(orow + (long long)Mo * a,
                        make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
         }
         tmem_ld16(dsrc + 32u, *reinterpret_cast<uint32_t(*)[16]>(r));
@@ -668,8 +674,8 @@ __device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& 
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const int a = my_a1 + 32 * (16 + i);
-            if (a < amax && c + (long long)M * a < n)
-                __stcs(orow + (long long)M * a,
+            if (a < amax && c + (long long)Mo * a < n)
+                __stcs(orow + (long long)Mo * a,
                        make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
         }
         g = gn;
@@ -694,14 +700,16 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const int N = 1 << log2N;
     const int M = N >> kLog2P2;
     const unsigned Nm = (unsigned)N - 1u;
-    const int n = S.n;
+    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
+    const int Mo = M / D;
+    const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
     const float inv = tc_prepass<KP, false>(P, R, S, tmem, s_red);
     const float s1 = 1.0f / (float)KP;
     const float fin = inv * (float)(KP * 1024);
 
-    const int ng = M / kTcCols;
+    const int ng = Mo / kTcCols;
     unsigned char* abuf = sm + h * kTcGbufBytes;        // DFT-stage A operand, 32 KB
     unsigned char* stage = abuf + kTcGbufBytes / 2;     // output staging, 32 KB
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
@@ -714,7 +722,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP, false>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+        build_b<KP, false>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
@@ -724,7 +732,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         }
     }
     const int tb = (wl >> 2) * 4;      // this warp drains phase-1 tiles tb .. tb + 3
-    const int amax = (n + M - 1) / M;  // stripes a that hold output samples
+    const int amax = (n + Mo - 1) / Mo;  // stripes a that hold output samples
     // stage-1 operand: this thread's rows 32 (j % 4) + lane of block j / 4, bytes 4 kb for kb = 8 qd + tb + 0..3
     const uint32_t a1_off = (uint32_t)((lane >> 3) * 1024 + (lane & 7) * 128 + ((((2 * qd + (tb >> 2)) ^ lane) & 7) << 4));
     // stage-2 operand: row 8 (a1 % 16) + wl of block a1 / 16, bytes 4 lane
@@ -739,7 +747,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
         tc_fence_after();
-        const int c0 = g * kTcCols;
+        const int c0 = g * kTcCols;  // first output column c' of the group (column D c0 of the row)
         {
             uint32_t pk[kTcCols][4];
 #pragma unroll
@@ -748,8 +756,8 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
                 tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
                 tmem_wait_ld();
                 const int k2 = lane + 32 * (8 * qd + tb + tt);
-                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)c0) & Nm), cscale(tg[lane], s1));
-                const float2 stp = twlo[k2];
+                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], s1));
+                const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
 #pragma unroll
                 for (int j = 0; j < kTcCols; j++) {
                     const float2 v = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
@@ -772,7 +780,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         }
         const int gn = g + 2;
         if (gn < ng) {
-            build_b<KP, false>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo);
+            build_b<KP, false>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
             fence_proxy_async_smem();
         }
         mbar_wait(mbar2_h, phase2, P.err);
@@ -832,7 +840,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
 #pragma unroll
             for (int a2 = 0; a2 < 32; a2++) {
                 const int a = my_a1 + 32 * a2;
-                if (a < amax && c + (long long)M * a < n) __stcs(orow + (long long)M * a, yv[a2]);
+                if (a < amax && c + (long long)Mo * a < n) __stcs(orow + (long long)Mo * a, yv[a2]);
             }
             g = gn;
             continue;
@@ -847,15 +855,15 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         if (tma) {
             fence_proxy_async_smem();
             half_bar(h);
-            const int n_full = n / M;
+            const int n_full = n / Mo;
             if (lane == 0 && wl >= 4) {
                 const int j = wl - 4;
                 if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
-            const int tail = n - n_full * M;
+            const int tail = n - n_full * Mo;
             if (ht < kTcCols && c0 + ht < tail && n_full < kP2) {
-                const long long idx = row0 + ht + (long long)M * n_full;
+                const long long idx = row0 + ht + (long long)Mo * n_full;
                 __stcs(reinterpret_cast<unsigned*>(outb) + idx,
                        *reinterpret_cast<const unsigned*>(stage + stage16_off(n_full, ht)));
             }
@@ -864,8 +872,8 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             for (int idx = ht; idx < kTcCols * kP2; idx += 256) {
                 const int w = idx & (kTcCols - 1);
                 const int a = idx >> 3;
-                if (c0 + w + (long long)M * a < n) {
-                    const long long o = row0 + w + (long long)M * a;
+                if (c0 + w + (long long)Mo * a < n) {
+                    const long long o = row0 + w + (long long)Mo * a;
                     __stcs(reinterpret_cast<unsigned*>(outb) + o,
                            *reinterpret_cast<const unsigned*>(stage + stage16_off(a, w)));
                 }

@@ -150,6 +150,21 @@ int fcwt_ccwt(fcwt_context* ctx, const float* input, int n, float fb, const floa
 int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const float* scales, int fn,
                      int threads, unsigned flags, int row_begin, int row_end, fcwt_plan** plan);
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type);
+/* Fused decimation epilogues (no reference counterpart: a caller of the
+ * reference decimates the [fn][n] output afterwards). Like fcwt_plan_create,
+ * but the plan produces rows row_begin, row_begin + row_stride, ... < row_end
+ * and in each row the samples t = 0, time_stride, 2 time_stride, ... < n:
+ * output [ceil((row_end - row_begin) / row_stride)][ceil(n / time_stride)].
+ * time_stride is a power of two; for padded lengths N > 8192 it must be at
+ * most N / 8192 (the four-step transform then skips the columns that are not
+ * kept, so decimation by D also divides the inverse-transform work by D).
+ * Every computed sample equals the undecimated transform's sample; the
+ * reused-bin semantics still follow all fn rows. */
+int fcwt_plan_create_strided(fcwt_context* ctx, int n, int is_complex, float fb, const float* scales, int fn,
+                             int threads, unsigned flags, int row_begin, int row_end, int row_stride,
+                             int time_stride, fcwt_plan** plan);
+/* Output shape (rows, samples per row) of a single-signal plan. */
+int fcwt_plan_output_shape(const fcwt_plan* plan, int* rows, int* cols);
 int fcwt_plan_destroy(fcwt_plan* plan);
 /* A caller-supplied wavelet: the reference's FCWT::cwt takes any Wavelet*
  * and uses the table its generate(N) fills (src/fcwt/fcwt.cpp:504-505,
