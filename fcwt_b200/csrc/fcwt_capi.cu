@@ -220,6 +220,9 @@ struct fcwt_context {
     };
     std::vector<CacheEntry> cache;
     unsigned long long use_clock = 0;
+    // host-output pipeline: copy stream, per-slot "rows done" / "block copied" events
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pipe_done[2] = {nullptr, nullptr}, pipe_copied[2] = {nullptr, nullptr};
     // profiling
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used, ev_free;
@@ -573,6 +576,7 @@ void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int,
 }
 
 int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type);
+int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* graph_jobs);
 
 // Enqueues the forward FFTs and the row engine for device-resident inputs and
 // outputs (no host synchronisation, so it can be captured into a graph).
@@ -582,9 +586,53 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     using namespace fcwt;
     fcwt_context* ctx = P->ctx;
     cudaStream_t st = ctx->stream;
-    const int nsig = (int)P->sig.size();
     if (P->doublesided && out_type != FCWT_OUT_C64)
         return fail(FCWT_ERR_UNSUPPORTED, "doublesided wavelets write complex64 outputs only");
+    int rc = enqueue_forward(P, din, graph_jobs);
+    if (rc) return rc;
+    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    const bool prof = ctx->profiling && allow_profiling;
+    if (prof) {
+        if (!ctx->ev_free.empty()) {
+            ev = ctx->ev_free.back();
+            ctx->ev_free.pop_back();
+        } else {
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
+        }
+        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
+    }
+    rc = enqueue_rows(P, P->sigs.as<SigDesc>(), dout, out_type);
+    if (rc) return rc;
+    if (P->doublesided) {
+        // the mirrored half: exp(-2 pi i t / N) conj(V), V the rows on the shifted spectrum
+        const PlanSignal& S = P->sig[0];
+        const float2* tw = P->tables[(size_t)S.table].tw.as<float2>();
+        FCWT_CUDA_TRY(launch_shift_spectrum(S.X.as<float2>(), S.sp.log2N, P->Xs.as<float2>(), st));
+        void* tmp_out[1] = {P->ds_tmp.p};
+        rc = enqueue_rows(P, P->sigs2.as<SigDesc>(), tmp_out, out_type);
+        if (rc) return rc;
+        FCWT_CUDA_TRY(launch_doublesided_combine(static_cast<float2*>(dout[0]), P->ds_tmp.as<float2>(),
+                                                 S.rows_out(), S.n_out(), S.dec, S.sp.log2N, tw,
+                                                 P->imag ? -1.0f : 1.0f, st));
+        ctx->kernel_launches += 2;
+    }
+    if (prof) {
+        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
+        ctx->ev_used.push_back(ev);
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return FCWT_OK;
+}
+
+// The forward FFTs of all signals of a plan into their spectra.
+int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* graph_jobs) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    cudaStream_t st = ctx->stream;
+    const int nsig = (int)P->sig.size();
     if (nsig == 1) {
         PlanSignal& S = P->sig[0];
         FCWT_CUDA_TRY(ctx->tmp.ensure((size_t)S.sp.N * sizeof(float2)));
@@ -615,40 +663,6 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
             off += g.second;
         }
     }
-    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
-    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
-    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
-    const bool prof = ctx->profiling && allow_profiling;
-    if (prof) {
-        if (!ctx->ev_free.empty()) {
-            ev = ctx->ev_free.back();
-            ctx->ev_free.pop_back();
-        } else {
-            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
-            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
-        }
-        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
-    }
-    int rc = enqueue_rows(P, P->sigs.as<SigDesc>(), dout, out_type);
-    if (rc) return rc;
-    if (P->doublesided) {
-        // the mirrored half: exp(-2 pi i t / N) conj(V), V the rows on the shifted spectrum
-        const PlanSignal& S = P->sig[0];
-        const float2* tw = P->tables[(size_t)S.table].tw.as<float2>();
-        FCWT_CUDA_TRY(launch_shift_spectrum(S.X.as<float2>(), S.sp.log2N, P->Xs.as<float2>(), st));
-        void* tmp_out[1] = {P->ds_tmp.p};
-        rc = enqueue_rows(P, P->sigs2.as<SigDesc>(), tmp_out, out_type);
-        if (rc) return rc;
-        FCWT_CUDA_TRY(launch_doublesided_combine(static_cast<float2*>(dout[0]), P->ds_tmp.as<float2>(),
-                                                 S.rows_out(), S.n_out(), S.dec, S.sp.log2N, tw,
-                                                 P->imag ? -1.0f : 1.0f, st));
-        ctx->kernel_launches += 2;
-    }
-    if (prof) {
-        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
-        ctx->ev_used.push_back(ev);
-    }
-    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     return FCWT_OK;
 }
 
@@ -716,6 +730,103 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
     return FCWT_OK;
 }
 
+// Host-output pipeline of a single-signal plan whose rows all run on the
+// tensor-core engine (rows independent of each other): rows are transformed
+// in blocks of about kPipeBlockBytes of output into two device staging slots,
+// and block b is copied to the host on a second stream while block b + 1 is
+// computed. Device staging is two blocks instead of the whole output, and
+// the transform overlaps the (PCIe-bound) copy.
+constexpr size_t kPipeBlockBytes = 256ull << 20;
+
+bool pipeline_applies(const fcwt_plan* P, size_t out_bytes) {
+    return P->sig.size() == 1 && P->n_items == 0 && P->n_tc == P->n_rows && !P->doublesided &&
+           out_bytes > kPipeBlockBytes;
+}
+
+int run_pipelined(fcwt_plan* P, const void* din, void* hout, int out_type) {
+    using namespace fcwt;
+    fcwt_context* ctx = P->ctx;
+    cudaStream_t st = ctx->stream;
+    const PlanSignal& S = P->sig[0];
+    const size_t esz = out_elem_bytes(out_type);
+    const size_t row_bytes = (size_t)S.n_out() * esz;
+    const int rows = P->n_rows;
+    const int blk = (int)std::max<size_t>(1, kPipeBlockBytes / row_bytes);
+    const int nblk = (rows + blk - 1) / blk;
+    FCWT_CUDA_TRY(ctx->out_stage.ensure(2 * (size_t)blk * row_bytes + 256));
+    if (!ctx->copy_stream) FCWT_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->pipe_done[i]) FCWT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->pipe_done[i], cudaEventDisableTiming));
+        if (!ctx->pipe_copied[i])
+            FCWT_CUDA_TRY(cudaEventCreateWithFlags(&ctx->pipe_copied[i], cudaEventDisableTiming));
+    }
+    const void* din_arr[1] = {din};
+    int rc = enqueue_forward(P, din_arr, nullptr);
+    if (rc) return rc;
+    FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), st));
+    FCWT_CUDA_TRY(ctx->counters.ensure((size_t)nblk * sizeof(unsigned)));
+    FCWT_CUDA_TRY(cudaMemsetAsync(ctx->counters.p, 0, (size_t)nblk * sizeof(unsigned), st));
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    const bool prof = ctx->profiling;
+    if (prof) {
+        if (!ctx->ev_free.empty()) {
+            ev = ctx->ev_free.back();
+            ctx->ev_free.pop_back();
+        } else {
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.first));
+            FCWT_CUDA_TRY(cudaEventCreate(&ev.second));
+        }
+        FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
+    }
+    const size_t slot_bytes = (size_t)blk * row_bytes;
+    for (int b = 0; b < nblk; b++) {
+        const int slot = b & 1;
+        const int r0 = b * blk, r1 = std::min(rows, r0 + blk);
+        char* stage = static_cast<char*>(ctx->out_stage.p) + (size_t)slot * slot_bytes;
+        // the slot is free once the copy of block b - 2 is done
+        if (b >= 2) FCWT_CUDA_TRY(cudaStreamWaitEvent(st, ctx->pipe_copied[slot], 0));
+        // rows r0.. of the plan write at out_off = r * row elements: shift the base so they land in the slot
+        char* base = stage - (size_t)r0 * row_bytes;
+        CUtensorMap omap;
+        std::memset(&omap, 0, sizeof(omap));
+        const int map_ok = out_type == FCWT_OUT_C64
+                               ? (encode_output_map(base, S.n_out(), S.sp.M / S.dec, r1, &omap) ? 1 : 0)
+                               : (encode_output_map16(base, S.n_out(), S.sp.M / S.dec, r1, &omap) ? 1 : 0);
+        TcParams tp;
+        std::memset(&tp, 0, sizeof(tp));
+        tp.sigs = P->sigs.as<SigDesc>();
+        tp.rows = P->rows.as<RowDesc>();
+        tp.row_list = P->tc_rows.as<int>() + r0;  // tc_rows lists the rows in order
+        tp.n_list = r1 - r0;
+        tp.stale_pool = P->pool.as<float>();
+        tp.wts = P->tc_wts.as<float>();
+        tp.counter = ctx->counters.as<unsigned>() + b;
+        tp.outs[0] = base;
+        tp.err = ctx->err.as<int>();
+        tp.tma_store = map_ok;
+        tp.c64_dft = tc_variant("FCWT_TC_C64_DFT", 0);
+        tp.direct16 = tc_variant("FCWT_TC_DIRECT16", 0);
+        FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(r1 - r0, ctx->num_sms)), st));
+        ctx->kernel_launches += 1;
+        FCWT_CUDA_TRY(cudaEventRecord(ctx->pipe_done[slot], st));
+        FCWT_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_done[slot], 0));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(hout) + (size_t)r0 * row_bytes, stage,
+                                      (size_t)(r1 - r0) * row_bytes, cudaMemcpyDeviceToHost, ctx->copy_stream));
+        FCWT_CUDA_TRY(cudaEventRecord(ctx->pipe_copied[slot], ctx->copy_stream));
+    }
+    if (prof) {
+        FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
+        ctx->ev_used.push_back(ev);
+    }
+    FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->err_host, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FCWT_CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+    FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (*ctx->err_host != 0)
+        return fail(FCWT_ERR_DEVICE, "row engine reported error bits " + std::to_string(*ctx->err_host));
+    return FCWT_OK;
+}
+
 // Runs a plan on host or device buffers: host inputs are staged in, host
 // outputs are copied back (and the call waits for them).
 int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs, int out_type) {
@@ -745,6 +856,17 @@ int plan_run_multi(fcwt_plan* P, const void* const* inputs, void* const* outputs
         out_off[(size_t)s] = out_total;
         out_bytes[(size_t)s] = (size_t)S.rows_out() * (size_t)S.n_out() * out_elem_bytes(out_type);
         if (!is_device_pointer(outputs[s])) out_total += (out_bytes[(size_t)s] + 255) & ~(size_t)255;
+    }
+    if (nsig == 1 && !is_device_pointer(outputs[0]) && pipeline_applies(P, out_bytes[0])) {
+        const PlanSignal& S = P->sig[0];
+        const void* din0 = inputs[0];
+        if (!is_device_pointer(inputs[0])) {
+            FCWT_CUDA_TRY(ctx->in_stage.ensure(in_total));
+            FCWT_CUDA_TRY(cudaMemcpyAsync(ctx->in_stage.p, inputs[0], (size_t)S.sp.n * (S.sp.is_complex ? 8 : 4),
+                                          cudaMemcpyHostToDevice, st));
+            din0 = ctx->in_stage.p;
+        }
+        return run_pipelined(P, din0, outputs[0], out_type);
     }
     if (in_total) FCWT_CUDA_TRY(ctx->in_stage.ensure(in_total));
     if (out_total) FCWT_CUDA_TRY(ctx->out_stage.ensure(out_total));
@@ -914,6 +1036,11 @@ int fcwt_context_destroy(fcwt_context* ctx) {
         cudaEventDestroy(ev.first);
         cudaEventDestroy(ev.second);
     }
+    for (int i = 0; i < 2; i++) {
+        if (ctx->pipe_done[i]) cudaEventDestroy(ctx->pipe_done[i]);
+        if (ctx->pipe_copied[i]) cudaEventDestroy(ctx->pipe_copied[i]);
+    }
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return FCWT_OK;
