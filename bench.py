@@ -630,14 +630,26 @@ def form_grad(steps: int, warmup: int, stream, check: bool = True) -> dict:
 
     ms_f = _timed(fwd, steps, warmup, stream)
     ms = _timed(step, steps, warmup, stream)
+    # the hand-written adjoint alone: backward of a kept forward with a fixed incoming gradient
+    y_keep = layer(x)
+    g_in = torch.randn(y_keep.shape, dtype=torch.complex64, device="cuda")
+
+    def adj():
+        x.grad = None
+        layer.zero_grad()
+        y_keep.backward(g_in, retain_graph=True)
+
+    ms_adj = _timed(adj, steps, warmup, stream)
+    del y_keep, g_in
     points = B * F * n
     res = {"metric": "scalogram points/s (forward + backward)", "value": points / (ms / 1e3),
            "unit": "points/s", "ms_per_step": ms,
            "config": {"workload": "grad_64x16384x128: batch 64 real f32 n=16384 fs=1000, learnable "
                                   "sigma (2.0) and 128 centre frequencies 2-200 Hz, loss MSE(|W|^2, target)",
                       "batch": B, "n": n, "fn": F},
-           "forward_ms": ms_f,
-           "note": "step = forward transform + loss + hand-written adjoint (signal, sigma, frequencies)"}
+           "forward_ms": ms_f, "adjoint_ms": ms_adj,
+           "note": "step = forward transform + loss + hand-written adjoint (signal, sigma, frequencies); "
+                   "adjoint_ms = the backward of a kept forward alone"}
     if check:
         from oracle.grad_ref import power_mse, ref_forward
 

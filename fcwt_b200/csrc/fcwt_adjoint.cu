@@ -91,6 +91,146 @@ __global__ void __launch_bounds__(kAdjThreads) k_adjoint_accum(const float2* __r
     }
 }
 
+// ---- fused row adjoint for N = 1024 M, M <= 16
+// One CTA per (signal b, chunk of kAdjFusedRows rows): each incoming gradient
+// row G[b,i] is transformed in shared memory (never written back), and its
+// spectrum is consumed on the spot. Forward DFT (sign -) of the zero-padded
+// row with t = c + M a, q = k2 + 1024 k1:
+//   Ghat[k2 + 1024 k1] = sum_c w_M^{-k1 c} w_N^{-k2 c} DFT1024_-(G[c + M a])[k2]
+// warp c runs the column DFT (as conj(DFT_+(conj))), the twiddled columns go
+// to shared memory, and each thread then runs the M-point DFTs of its two k2
+// values and accumulates, for its bins q < N/2, H[b][q] (in registers across
+// the chunk's rows) and the sigma / frequency partial sums.
+constexpr int kAdjFusedThreads = 512;
+constexpr int kAdjFusedRows = 8;
+constexpr int kAdjColPitch = kP2 + 1;  // column pitch (float2) of the shared buffer: conflict-free rows and columns
+
+template <int M>
+__global__ void __launch_bounds__(kAdjFusedThreads, 1)
+    k_adjoint_rows(const float2* __restrict__ G, const float2* __restrict__ Xs, const AdjRow* __restrict__ rows,
+                   int n, int fn, const float2* __restrict__ tw, float cb, float amp, float inv_sigma,
+                   float2* __restrict__ H, double* __restrict__ acc_sigma, double* __restrict__ acc_f) {
+    constexpr int N = kP2 * M;
+    constexpr int HALF = N / 2;
+    constexpr int LOGM = ilog2c(M);
+    constexpr int KH = M >= 2 ? M / 2 : 1;  // bins per k2 below N/2
+    extern __shared__ __align__(16) float2 adj_sm[];
+    float2* S = adj_sm;                              // [M][kAdjColPitch]
+    float2* t2 = adj_sm + M * kAdjColPitch;          // 32 x 32 DFT twiddles
+    float2* twlo = t2 + kP2;                         // w_N^j, j < 1024
+    float2* twhi = twlo + kP2;                       // w_N^{1024 j}, j < M
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int b = blockIdx.y;
+    const int i0 = blockIdx.x * kAdjFusedRows;
+    const int nr = min(kAdjFusedRows, fn - i0);
+    for (int j = tid; j < kP2; j += kAdjFusedThreads) {
+        const int a = j >> 5, l = j & 31;
+        double sn, cs;
+        sincospi(2.0 * (double)((a * l) & 1023) / 1024.0, &sn, &cs);
+        t2[j] = make_float2((float)cs, (float)sn);
+        twlo[j] = tw[j];
+    }
+    if (tid < M) twhi[tid] = M > 1 ? tw[kP2 + tid] : make_float2(1.0f, 0.0f);
+    const unsigned Nm = (unsigned)N - 1u;
+    float2 h[2][KH];
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+        for (int k = 0; k < KH; k++) h[u][k] = make_float2(0.0f, 0.0f);
+    float dsig = 0.0f;
+    __shared__ float s_df[kAdjFusedRows];  // per-row dL/df partial sums of the CTA
+    if (tid < kAdjFusedRows) s_df[tid] = 0.0f;
+    const float2* __restrict__ Xb = Xs + (size_t)b * N;
+    __syncthreads();
+    for (int r = 0; r < nr; r++) {
+        const int i = i0 + r;
+        const float2* __restrict__ g = G + ((size_t)b * fn + i) * (size_t)n;
+        // (a) the row, conjugated, column-major: S[c][a] = conj(G[c + M a]), zero past n
+        for (int t = tid; t < N; t += kAdjFusedThreads) {
+            const float2 v = t < n ? __ldcs(g + t) : make_float2(0.0f, 0.0f);
+            S[(t & (M - 1)) * kAdjColPitch + (t >> LOGM)] = make_float2(v.x, -v.y);
+        }
+        __syncthreads();
+        // (b) column DFTs, twiddle w_N^{-k2 c}, back into the column
+        if (warp < M) {
+            float2* col = S + warp * kAdjColPitch;
+            float2 x[32];
+#pragma unroll
+            for (int m = 0; m < 32; m++) x[m] = col[lane + 32 * m];
+            __syncwarp();
+            dft1024_warp_xor(x, lane, col, t2);
+#pragma unroll
+            for (int hh = 0; hh < 32; hh++) {
+                const int k2 = lane + 32 * hh;
+                const unsigned e = ((unsigned)k2 * (unsigned)warp) & Nm;
+                const float2 w = cmul(twlo[e & 1023u], twhi[e >> 10]);
+                // conj(x) * conj(w)
+                const float2 y = make_float2(x[hh].x * w.x - x[hh].y * w.y, -(x[hh].x * w.y + x[hh].y * w.x));
+                col[k2] = y;
+            }
+        }
+        __syncthreads();
+        // (c) M-point DFTs (sign -) across the columns; accumulate bins q < N/2
+        const AdjRow rc = rows[i];
+        float dfl = 0.0f;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int k2 = tid + kAdjFusedThreads * u;
+            float2 z[M];
+#pragma unroll
+            for (int c = 0; c < M; c++) z[c] = S[c * kAdjColPitch + k2];
+            fft_reg<M, -1>(z);
+#pragma unroll
+            for (int k1 = 0; k1 < KH; k1++) {
+                const int q = k2 + kP2 * k1;
+                if (q < HALF) {
+                    const float qf = (float)q;
+                    const float uu = rc.ca * qf - cb;
+                    const float gw = amp * expf(-0.5f * uu * uu);
+                    const float2 gh = z[k1];
+                    h[u][k1].x += gw * gh.x;
+                    h[u][k1].y += gw * gh.y;
+                    const float2 xq = __ldg(Xb + q);
+                    const float re = xq.x * gh.x + xq.y * gh.y;
+                    dsig += -gw * uu * uu * inv_sigma * re;
+                    dfl += gw * uu * rc.dfdq * qf * re;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dfl += __shfl_xor_sync(0xffffffffu, dfl, o);
+        if (lane == 0) atomicAdd(&s_df[r], dfl);
+        __syncthreads();
+    }
+    // H[b][q] += h (only bins this chunk touched), then the parameter sums
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        const int k2 = tid + kAdjFusedThreads * u;
+#pragma unroll
+        for (int k1 = 0; k1 < KH; k1++) {
+            const int q = k2 + kP2 * k1;
+            if (q < HALF && (h[u][k1].x != 0.0f || h[u][k1].y != 0.0f)) {
+                float* hp = reinterpret_cast<float*>(H + (size_t)b * N + q);
+                atomicAdd(hp, h[u][k1].x);
+                atomicAdd(hp + 1, h[u][k1].y);
+            }
+        }
+    }
+    __shared__ float red[kAdjFusedThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dsig += __shfl_xor_sync(0xffffffffu, dsig, o);
+    if (lane == 0) red[warp] = dsig;
+    __syncthreads();
+    if (tid == 0) {
+        double sacc = 0.0;
+        for (int w = 0; w < kAdjFusedThreads / 32; w++) sacc += (double)red[w];
+        atomicAdd(acc_sigma, sacc);
+    }
+    if (tid < nr) atomicAdd(acc_f + i0 + tid, (double)s_df[tid]);
+}
+
 // grad_x[b][t] = scale * Re(Y[b][t]) for t < n.
 __global__ void k_take_real(const float2* __restrict__ Y, long long Nstride, int n, float scale,
                             float* __restrict__ gx) {
@@ -119,5 +259,37 @@ cudaError_t launch_take_real(const float2* Y, long long Nstride, int n, int batc
 }
 
 int adjoint_rows_per_pass() { return dev::kAdjMaxRows; }
+
+size_t adjoint_fused_smem(int M) { return sizeof(float2) * ((size_t)M * dev::kAdjColPitch + 2 * kP2 + 16); }
+
+// The fused row adjoint for N = 1024 M, M in {1, 2, 4, 8, 16}; returns
+// cudaErrorInvalidValue for other N (the caller then uses the FFT passes).
+cudaError_t launch_adjoint_rows(const float2* G, const float2* Xs, const void* rows, int n, int log2N, int fn,
+                                int batch, const float2* tw, float cb, float amp, float inv_sigma, float2* H,
+                                double* acc_sigma, double* acc_f, cudaStream_t st) {
+    const int M = log2N >= kLog2P2 ? 1 << (log2N - kLog2P2) : 0;
+    if (M < 1 || M > 16) return cudaErrorInvalidValue;
+    const dim3 grid((fn + dev::kAdjFusedRows - 1) / dev::kAdjFusedRows, batch);
+    const size_t sm = adjoint_fused_smem(M);
+    const auto* r = static_cast<const dev::AdjRow*>(rows);
+    cudaError_t e = cudaSuccess;
+#define FCWT_ADJ_CASE(MM)                                                                                   \
+    case MM:                                                                                                \
+        e = cudaFuncSetAttribute(dev::k_adjoint_rows<MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+        if (e != cudaSuccess) return e;                                                                     \
+        dev::k_adjoint_rows<MM><<<grid, dev::kAdjFusedThreads, sm, st>>>(G, Xs, r, n, fn, tw, cb, amp, inv_sigma, \
+                                                                          H, acc_sigma, acc_f);             \
+        break;
+    switch (M) {
+        FCWT_ADJ_CASE(1)
+        FCWT_ADJ_CASE(2)
+        FCWT_ADJ_CASE(4)
+        FCWT_ADJ_CASE(8)
+        FCWT_ADJ_CASE(16)
+        default: return cudaErrorInvalidValue;
+    }
+#undef FCWT_ADJ_CASE
+    return cudaGetLastError();
+}
 
 }  // namespace fcwt

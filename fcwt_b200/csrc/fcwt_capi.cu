@@ -38,6 +38,9 @@ cudaError_t launch_adjoint_accum(const float2* Xs, const float2* Gh, float2* H, 
 cudaError_t launch_take_real(const float2* Y, long long Nstride, int n, int batch, float scale, float* gx,
                              cudaStream_t st);
 int adjoint_rows_per_pass();
+cudaError_t launch_adjoint_rows(const float2* G, const float2* Xs, const void* rows, int n, int log2N, int fn,
+                                int batch, const float2* tw, float cb, float amp, float inv_sigma, float2* H,
+                                double* acc_sigma, double* acc_f, cudaStream_t st);
 cudaError_t engine_configure();
 cudaError_t engine_blocks_per_sm(int* out);
 cudaError_t launch_engine(const EngineParams& p, int grid, cudaStream_t st);
@@ -1576,7 +1579,15 @@ int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch
     jo += batch;
     // rows in chunks: Ghat = FFT(G), accumulate H and the parameter sums
     const float2* G = static_cast<const float2*>(grad_out);
-    for (int c = 0; c < nchunks; c++) {
+    const bool fused = log2N >= kLog2P2 && log2N <= kLog2P2 + 4;  // N = 1024 .. 16384: one kernel, in SMEM
+    if (fused) {
+        FCWT_CUDA_TRY(launch_adjoint_rows(G, ctx->adj_x.as<float2>(), ctx->adj_rows.p, n, log2N, fn, batch, tw,
+                                          (float)(two_pi * fb), host::mother_norm(), 1.0f / fb,
+                                          ctx->adj_h.as<float2>(), ctx->adj_acc.as<double>(),
+                                          ctx->adj_acc.as<double>() + 1, st));
+        ctx->kernel_launches += 1;
+    }
+    for (int c = 0; c < (fused ? 0 : nchunks); c++) {
         const int i0 = c * RP;
         const int nr = std::min(RP, fn - i0);
         for (int b = 0; b < batch; b++) {

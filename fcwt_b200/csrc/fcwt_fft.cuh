@@ -91,6 +91,23 @@ __device__ __forceinline__ void fft_reg(float2 (&x)[K]) {
     }
 }
 
+// Warp-level 1024-point DFT (sign +) with an XOR-swizzled 32 x 32 transpose
+// buffer (8 KB): on entry lane l holds x[m] = G[l + 32 m]; on exit lane l
+// holds x[h] = Y[l + 32 h]. t2[a * 32 + l] = exp(+2 pi i a l / 1024).
+__device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, float2* __restrict__ tb,
+                                                 const float2* __restrict__ t2) {
+    fft_reg<32, +1>(x);
+#pragma unroll
+    for (int a = 1; a < 32; a++) x[a] = cmul(x[a], t2[a * 32 + lane]);
+#pragma unroll
+    for (int a = 0; a < 32; a++) tb[a * 32 + (lane ^ a)] = x[a];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 32; k++) x[k] = tb[lane * 32 + (k ^ lane)];
+    __syncwarp();
+    fft_reg<32, +1>(x);
+}
+
 // w_N^e from the two-level table of a transform length N = 2^log2N:
 // tw[0..1023] = w_N^j, tw[1024 + j] = w_N^{1024 j}. SIGN < 0 conjugates.
 __device__ __forceinline__ float2 tw_lookup(const float2* __restrict__ tw, int log2N, unsigned e) {

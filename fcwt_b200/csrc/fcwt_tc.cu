@@ -151,23 +151,6 @@ __device__ __forceinline__ void half_bar(int h) { asm volatile("bar.sync %0, 256
 
 __device__ __forceinline__ uint32_t h2bits(__half2 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
-// Warp-level 1024-point DFT (sign +) with an XOR-swizzled 32 x 32 transpose
-// buffer (8 KB): on entry lane l holds x[m] = G[l + 32 m]; on exit lane l
-// holds x[h] = Y[l + 32 h].
-__device__ __forceinline__ void dft1024_warp_xor(float2 (&x)[32], int lane, float2* __restrict__ tb,
-                                                 const float2* __restrict__ t2) {
-    fft_reg<32, +1>(x);
-#pragma unroll
-    for (int a = 1; a < 32; a++) x[a] = cmul(x[a], t2[a * 32 + lane]);
-#pragma unroll
-    for (int a = 0; a < 32; a++) tb[a * 32 + (lane ^ a)] = x[a];
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < 32; k++) x[k] = tb[lane * 32 + (k ^ lane)];
-    __syncwarp();
-    fft_reg<32, +1>(x);
-}
-
 // B operand of group g: rows j (Re G) and 8 + j (Im G) of column c = 8 g + j,
 // K index 2 k1 + {re, im}; byte offset of element (n, k) in the canonical
 // K-major layout: (k / 16) * 512 + (n / 8) * 256 + ((k / 8) % 2) * 128 +

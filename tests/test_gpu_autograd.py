@@ -66,6 +66,22 @@ def test_forward_and_gradients(n, F, norm):
     h = 1e-6
     fd_sig = (L_at(sig0 + h, f0) - L_at(sig0 - h, f0)) / (2 * h)
     assert abs(float(sigma.grad) - fd_sig) <= 1e-4 * abs(fd_sig) + 1e-10
+    # dL/dx along random unit directions v: <dL/dx, v> against central differences
+    # of the float64 operator, L(x + h v) - L(x - h v) over 2h
+    rngd = np.random.default_rng(n + 1)
+    for _ in range(3):
+        v = torch.from_numpy(rngd.standard_normal((B, n)))
+        v /= torch.linalg.vector_norm(v)
+        hx = 1e-4 * float(torch.linalg.vector_norm(xr.detach()))
+        with torch.no_grad():
+            Lp = float(loss_fn(ref_forward(xr.detach() + hx * v, torch.tensor(sig0, dtype=torch.float64),
+                                           torch.tensor(f0, dtype=torch.float64), fs, norm), target))
+            Lm = float(loss_fn(ref_forward(xr.detach() - hx * v, torch.tensor(sig0, dtype=torch.float64),
+                                           torch.tensor(f0, dtype=torch.float64), fs, norm), target))
+        fd_x = (Lp - Lm) / (2 * hx)
+        got_x = float((gx * v).sum())
+        scale_x = float(torch.linalg.vector_norm(gxr))
+        assert abs(got_x - fd_x) <= 1e-4 * max(abs(fd_x), 1e-3 * scale_x), (got_x, fd_x)
     k = F // 2
     fp, fm = f0.copy(), f0.copy()
     hf = 1e-6 * f0[k]
