@@ -13,9 +13,10 @@
 # for the daughter loop, asserts compiled out (Release). The reference source
 # omits <cassert>/<cstring>, hence the -include flags.
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   (default: $FCWT_REFERENCE_ROOT, else /root/reference)
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${FCWT_REFERENCE_ROOT:-/root/reference}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/fcwt/fcwt.cpp" ]; then

@@ -54,12 +54,15 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_reference(reference_root: str = "/root/reference") -> str | None:
+def build_reference(reference_root: str | None = None) -> str | None:
     """Build oracle/_ref/libfcwt_ref.so from the reference sources, when they
-    are present on this machine. Returns the library path or None."""
-    if not os.path.isfile(os.path.join(reference_root, "src", "fcwt", "fcwt.cpp")):
+    are present on this machine. The source tree is `reference_root`, else
+    $FCWT_REFERENCE_ROOT, else the default of oracle/build_ref.sh. Returns the
+    library path, or None when neither the sources nor a built library exist."""
+    root = reference_root or os.environ.get("FCWT_REFERENCE_ROOT")
+    args = ["bash", os.path.join(HERE, "build_ref.sh")] + ([root] if root else [])
+    if subprocess.run(args, capture_output=True).returncode != 0:
         return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
-    subprocess.check_call(["bash", os.path.join(HERE, "build_ref.sh"), reference_root])
     return REF_LIB_PATH
 
 
