@@ -27,6 +27,7 @@ FCWT_CONTINUOUS = 1 << 3
 FCWT_STRICT = 1 << 4
 FCWT_IMAG_FREQUENCY = 1 << 5
 FCWT_DOUBLESIDED = 1 << 6
+FCWT_COMPAT_ALIGN = 1 << 7
 
 FCWT_OUT_C64 = 0
 FCWT_OUT_BF16 = 1

@@ -260,13 +260,15 @@ class FCWT:
     the result: it sets the per-scale truncation length (fcwt.cpp:213-214)."""
 
     def __init__(self, pwav, pthreads, puse_optimalization_schemes, puse_normalization, device: int = 0,
-                 strict=None):
+                 strict=None, compat_align_shift: bool = False):
         self.wavelet = pwav
         self.threads = _as_int("pthreads", pthreads)
         self.use_optimalization_schemes = bool(puse_optimalization_schemes)
         self.use_normalization = bool(puse_normalization)
         self.device = device
-        self.flags = (FCWT_NORM if self.use_normalization else 0) | (FCWT_STRICT if _strict(strict) else 0)
+        # compat_align_shift: reproduce the reference's odd-n row shift (src/fcwt/fcwt.cpp:418-426)
+        self.flags = (FCWT_NORM if self.use_normalization else 0) | (FCWT_STRICT if _strict(strict) else 0) | \
+            (_lib.FCWT_COMPAT_ALIGN if compat_align_shift else 0)
 
     # -- tuning files (src/fcwt/fcwt.cpp:313-393)
     def create_FFT_optimization_plan(self, pmaxsize, poptimizationflags) -> None:
@@ -442,7 +444,7 @@ class Plan:
     def __init__(self, n: int, scales, fb: float = 2.0, threads: int = 1, norm: bool = True,
                  complex_input: bool = False, rows: tuple[int, int] | None = None, device: int = 0,
                  exact_support: bool = False, scalar_trunc: bool = False, row_stride: int = 1,
-                 time_stride: int = 1):
+                 time_stride: int = 1, compat_align_shift: bool = False):
         self.ctx = _lib.context(device)
         self.device = device
         self.scales = _scales_array(scales).copy()
@@ -451,7 +453,7 @@ class Plan:
         self.rows = rows if rows is not None else (0, self.fn)
         self.complex_input = complex_input
         flags = (FCWT_NORM if norm else 0) | (FCWT_EXACT_SUPPORT if exact_support else 0) | \
-            (FCWT_SCALAR_TRUNC if scalar_trunc else 0)
+            (FCWT_SCALAR_TRUNC if scalar_trunc else 0) | (_lib.FCWT_COMPAT_ALIGN if compat_align_shift else 0)
         h = ctypes.c_void_p()
         if row_stride == 1 and time_stride == 1:
             _lib.call("fcwt_plan_create", self.ctx.handle, self.n, 1 if complex_input else 0, ctypes.c_float(fb),

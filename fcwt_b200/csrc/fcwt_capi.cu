@@ -50,6 +50,8 @@ cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const in
                               const float* pool, float* wts, cudaStream_t st);
 cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st);
 cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStream_t st);
+cudaError_t launch_align_spill(const SigDesc* sigs, const RowDesc* rows, const int* list, int nlist,
+                               const float* pool, float2* out, int n, float extra, cudaStream_t st);
 cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long rows, int n, int dec, int log2N,
                                        const float2* tw, float sgn, cudaStream_t st);
 }  // namespace fcwt
@@ -270,6 +272,9 @@ struct fcwt_plan {
     std::vector<float> custom_mother;  // caller's wavelet table (N floats), empty for Morlet(fb)
     bool imag = false;         // wavelet with imag_frequency: every product times i
     bool doublesided = false;  // wavelet with doublesided: second pass on the shifted spectrum
+    bool compat_align = false; // reference's odd-n row shift (FCWT_COMPAT_ALIGN)
+    DevBuf shifted;            // compat_align: the rows written one sample to the right
+    int n_shifted = 0;
     DevBuf Xs, sigs2, ds_tmp;  // doublesided: shifted spectrum, its signal descriptor, second-pass rows
     int slots = 0;
     long long slot_elems = 0;
@@ -308,6 +313,7 @@ void plan_free(fcwt_plan* p) {
     p->Xs.release();
     p->sigs2.release();
     p->ds_tmp.release();
+    p->shifted.release();
     if (p->jobs_host) cudaFreeHost(p->jobs_host);
     delete p;
 }
@@ -342,6 +348,7 @@ int plan_build(fcwt_plan* P) {
     std::vector<int> wts_rows;        // rows that own a weight-table entry
     std::map<std::array<uint32_t, 12>, long long> wts_owner;
     std::vector<Item> items;
+    std::vector<int> compat_rows;     // compat_align: shifted rows (descriptor indices)
     int max_two_phase_log2N = 0;
     for (int s = 0; s < nsig; s++) {
         PlanSignal& S = P->sig[(size_t)s];
@@ -375,6 +382,12 @@ int plan_build(fcwt_plan* P) {
             d.dec = S.dec;
             d.n_out = S.n_out();
             d.out_off = (long long)ro * d.n_out;
+            if (P->compat_align && (sp.n & 1) && (r & 1) && r < sp.rows.size() - 1) {
+                // written through std::align: one sample to the right, n - 1 samples
+                d.out_off += 1;
+                d.n_out -= 1;
+                compat_rows.push_back((int)rows.size());
+            }
             d.out_scale = out_scale;
             d.out_row = ro;
             d.mode = (sp.flags & kFlagContinuous) ? 1 : 0;
@@ -524,6 +537,12 @@ int plan_build(fcwt_plan* P) {
         FCWT_CUDA_TRY(cudaStreamSynchronize(st));
         owners.release();
     }
+    if (!compat_rows.empty()) {
+        FCWT_CUDA_TRY(P->shifted.ensure(compat_rows.size() * sizeof(int)));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->shifted.p, compat_rows.data(), compat_rows.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, st));
+    }
+    P->n_shifted = (int)compat_rows.size();
     if (P->doublesided) {
         const PlanSignal& S = P->sig[0];
         FCWT_CUDA_TRY(P->Xs.ensure((size_t)S.sp.N * sizeof(float2)));
@@ -591,6 +610,8 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
     cudaStream_t st = ctx->stream;
     if (P->doublesided && out_type != FCWT_OUT_C64)
         return fail(FCWT_ERR_UNSUPPORTED, "doublesided wavelets write complex64 outputs only");
+    if (P->compat_align && out_type != FCWT_OUT_C64)
+        return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN writes complex64 outputs only");
     int rc = enqueue_forward(P, din, graph_jobs);
     if (rc) return rc;
     FCWT_CUDA_TRY(ctx->err.ensure(sizeof(int)));
@@ -621,6 +642,16 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
                                                  S.rows_out(), S.n_out(), S.dec, S.sp.log2N, tw,
                                                  P->imag ? -1.0f : 1.0f, st));
         ctx->kernel_launches += 2;
+    }
+    if (P->n_shifted > 0) {
+        const PlanSignal& S = P->sig[0];
+        if (((uintptr_t)dout[0] & 15) != 0)
+            return fail(FCWT_ERR_INVALID, "FCWT_COMPAT_ALIGN needs a 16-byte aligned output");
+        const float extra = (S.sp.flags & kFlagNorm) ? 1.0f / (float)S.sp.N : 1.0f;
+        FCWT_CUDA_TRY(launch_align_spill(P->sigs.as<SigDesc>(), P->rows.as<RowDesc>(), P->shifted.as<int>(),
+                                         P->n_shifted, P->pool.as<float>(), static_cast<float2*>(dout[0]), S.sp.n,
+                                         extra, st));
+        ctx->kernel_launches += 1;
     }
     if (prof) {
         FCWT_CUDA_TRY(cudaEventRecord(ev.second, st));
@@ -743,7 +774,7 @@ constexpr size_t kPipeBlockBytes = 256ull << 20;
 
 bool pipeline_applies(const fcwt_plan* P, size_t out_bytes) {
     return P->sig.size() == 1 && P->n_items == 0 && P->n_tc == P->n_rows && !P->doublesided &&
-           out_bytes > kPipeBlockBytes;
+           P->n_shifted == 0 && out_bytes > kPipeBlockBytes;
 }
 
 int run_pipelined(fcwt_plan* P, const void* din, void* hout, int out_type) {
@@ -1208,6 +1239,11 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
     P->sig.resize(1);
     P->sig[0].rb = row_begin;
     P->sig[0].re = row_end;
+    P->compat_align = (flags & FCWT_COMPAT_ALIGN) != 0;
+    if (P->compat_align && (row_begin != 0 || row_end != fn)) {
+        delete P;
+        return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN applies to whole plans (all rows)");
+    }
     std::string err;
     if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sig[0].sp, err)) {
         delete P;
@@ -1234,6 +1270,7 @@ int fcwt_plan_create_strided(fcwt_context* ctx, int n, int is_complex, float fb,
     if (row_stride < 1) return fail(FCWT_ERR_INVALID, "row_stride must be >= 1");
     if (time_stride < 1 || (time_stride & (time_stride - 1)))
         return fail(FCWT_ERR_INVALID, "time_stride must be a power of two >= 1");
+    if (flags & FCWT_COMPAT_ALIGN) return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN with decimation");
     if (fn < 0 || n < 0) return fail(FCWT_ERR_INVALID, "negative size");
     if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
     if (row_begin < 0 || row_end > fn || row_begin > row_end)
@@ -1303,6 +1340,11 @@ int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const floa
     P->custom_mother.assign(mother, mother + N);
     P->imag = (flags & FCWT_IMAG_FREQUENCY) != 0;
     P->doublesided = (flags & FCWT_DOUBLESIDED) != 0;
+    P->compat_align = (flags & FCWT_COMPAT_ALIGN) != 0;
+    if (P->compat_align && (P->doublesided || row_begin != 0 || row_end != fn)) {
+        delete P;
+        return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN applies to whole plans of single-sided wavelets");
+    }
     P->sig.resize(1);
     P->sig[0].rb = row_begin;
     P->sig[0].re = row_end;

@@ -724,6 +724,49 @@ __global__ void k_doublesided_combine(float2* __restrict__ out, const float2* __
 }
 }  // namespace dev
 
+// ---- the reference's odd-n row shift (compat mode, src/fcwt/fcwt.cpp:418-445)
+// A shifted row r keeps at element 0 what row r - 1's inverse FFT wrote past
+// its n samples, sample n of that row, normalised by both rows' fft_normalize:
+//   out[r][0] = extra * sum_q Z_{r-1}[q] exp(2 pi i q n / N)
+// (Z includes the first 1/N when normalising; extra is the second).
+namespace dev {
+__global__ void k_align_spill(const SigDesc* __restrict__ sigs, const RowDesc* __restrict__ rows,
+                              const int* __restrict__ list, const float* __restrict__ pool, float2* __restrict__ out,
+                              int n, float extra) {
+    const int r = list[blockIdx.x];
+    const RowDesc R = rows[r - 1];
+    const SigDesc S = sigs[R.sig];
+    const int N = 1 << S.log2N;
+    const float nm1 = (float)N - 1.0f;
+    float2 acc = make_float2(0.0f, 0.0f);
+    for (int q = R.lo + threadIdx.x; q < R.hi; q += blockDim.x) {
+        const float2 z = bin_value(R, S, pool, nm1, q);
+        const float2 w = tw_lookup(S.tw, S.log2N, (unsigned)(((long long)q * n) & (N - 1)));
+        acc = cadd(acc, cmul(z, w));
+    }
+    __shared__ float2 red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float2 s = make_float2(0.0f, 0.0f);
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = cadd(s, red[w]);
+        out[(long long)r * n] = make_float2(s.x * extra, s.y * extra);
+    }
+}
+}  // namespace dev
+
+cudaError_t launch_align_spill(const SigDesc* sigs, const RowDesc* rows, const int* list, int nlist,
+                               const float* pool, float2* out, int n, float extra, cudaStream_t st) {
+    if (nlist <= 0) return cudaSuccess;
+    dev::k_align_spill<<<nlist, 256, 0, st>>>(sigs, rows, list, pool, out, n, extra);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_shift_spectrum(const float2* X, int log2N, float2* J, cudaStream_t st) {
     const int N = 1 << log2N;
     dev::k_shift_spectrum<<<std::max(1, std::min(1184, (N + 255) / 256)), 256, 0, st>>>(X, N, J);

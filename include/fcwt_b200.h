@@ -54,6 +54,12 @@ extern "C" {
 #define FCWT_IMAG_FREQUENCY (1u << 5) /* every product is i * mother[idx] * Ihat[q] */
 #define FCWT_DOUBLESIDED (1u << 6)    /* bins b in [N - proc, N) are also written, with weight
                                          mother[idx(N - 1 - b)] on the mirrored spectrum (complex64 output) */
+#define FCWT_COMPAT_ALIGN (1u << 7)   /* reproduce the reference's odd-n row shift (src/fcwt/fcwt.cpp:418-426):
+                                         its inverse FFT writes through std::align(16, ...), so with a 16-byte
+                                         aligned output a row i < fn - 1 whose start is 8 mod 16 (odd n, odd i)
+                                         holds y_i[t - 1] at t >= 1 and, at t = 0, the previous row's sample
+                                         n left there, normalised twice. Complex64 output, whole plans
+                                         (all rows, no decimation), 16-byte aligned output only */
 
 /* ---- output element types */
 #define FCWT_OUT_C64 0   /* interleaved float32 (re, im): std::complex<float>      */

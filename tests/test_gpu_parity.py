@@ -261,3 +261,34 @@ def test_device_weights_equal_reference_daughter_product(fcwt, golden, mode):
             assert np.array_equal(np.round(W[:, :half].real).astype(np.int32), golden[f"dw_{k}"]), (k, mode)
     finally:
         c.set_engine(_lib.FCWT_ENGINE_AUTO)
+
+
+@pytest.mark.parametrize("n", [1001, 9999, 40001])
+@pytest.mark.parametrize("norm", [True, False])
+def test_compat_align_shift_reproduces_reference_rows(fcwt, oracle, reference, n, norm):
+    """With compat_align_shift the odd-n output equals the reference's own
+    output row for row, including the rows its std::align writes one sample to
+    the right and their element 0 (the previous row's sample n, normalised
+    twice): src/fcwt/fcwt.cpp:418-445."""
+    import torch
+
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal(n) + np.sin(np.arange(n) * 0.02)).astype(np.float32)
+    sc = oracle.scales(LOGSCALES, 1000, 2.0, 400.0, 9)
+    want = reference.cwt(x, sc, 2.0, 1000, 2, norm)
+    assert want.ctypes.data % 16 == 0
+    got = np.zeros_like(want)
+    fcwt.FCWT(fcwt.Morlet(2.0), 2, False, norm, compat_align_shift=True).cwt(x, sc, got)
+    for i in range(sc.size):
+        assert rel_l2(got[i], want[i]) < 1e-5, i
+        assert abs(got[i, 0] - want[i, 0]) <= 1e-5 * np.abs(want[i]).max() + 1e-30, i
+    # device buffers: same
+    dev = torch.empty((sc.size, n), dtype=torch.complex64, device="cuda")
+    fcwt.FCWT(fcwt.Morlet(2.0), 2, False, norm, compat_align_shift=True).cwt(torch.from_numpy(x).cuda(), sc, dev)
+    torch.cuda.synchronize()
+    assert rel_l2(dev.cpu().numpy(), want) < 1e-5
+    # without the mode, rows are clean (unshifted)
+    clean = np.zeros_like(want)
+    fcwt.FCWT(fcwt.Morlet(2.0), 2, False, norm).cwt(x, sc, clean)
+    ref64 = oracle.cwt_fp64(x, sc, 2.0, 2, norm)
+    assert rel_l2(clean, ref64) < 1e-5
