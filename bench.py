@@ -418,6 +418,19 @@ def plain_forms(plan, xd, out, sel, out_rows, ms_step, fn, N, stream, args) -> d
                           "speedup_vs_complex64": ms_step / ms_p,
                           "rel_l2_vs_fp64_abs2": rel_l2(pw, np.abs(fp64) ** 2)}
     del outp
+    # fused decimation: every 16th sample of every row (the transform skips the other columns)
+    D = 16
+    pd = fcwt.Plan(N_SAMPLES, plan.scales, fb=SIGMA, threads=THREADS, norm=True, time_stride=D)
+    outd = torch.empty(pd.out_shape, dtype=torch.complex64, device=dev)
+    ms_d = _timed(lambda: pd.execute(xd, outd, stream=stream), args.steps, args.warmup, stream)
+    gd = outd[tsel].cpu().numpy()
+    forms["decimated_t16"] = {"value": fn * pd.out_shape[1] / (ms_d / 1e3), "unit": "output points/s",
+                              "ms_per_step": ms_d, "speedup_vs_complex64": ms_step / ms_d,
+                              "output_shape": list(pd.out_shape),
+                              "rel_l2_vs_full_transform": rel_l2(gd, out_rows[:, ::D]),
+                              "rel_l2_vs_fp64": rel_l2(gd, fp64[:, ::D])}
+    del outd
+    pd.close()
     return forms
 
 
