@@ -820,8 +820,9 @@ int run_pipelined(fcwt_plan* P, const void* din, void* hout, int out_type) {
         char* stage = static_cast<char*>(ctx->out_stage.p) + (size_t)slot * slot_bytes;
         // the slot is free once the copy of block b - 2 is done
         if (b >= 2) FCWT_CUDA_TRY(cudaStreamWaitEvent(st, ctx->pipe_copied[slot], 0));
-        // rows r0.. of the plan write at out_off = r * row elements: shift the base so they land in the slot
-        char* base = stage - (size_t)r0 * row_bytes;
+        // rows r0.. of the plan write at out_off = r * row elements: shift the base so they land in the
+        // slot (an address below the slot that no access uses; only base + out_off is dereferenced)
+        char* base = reinterpret_cast<char*>(reinterpret_cast<uintptr_t>(stage) - (uintptr_t)r0 * row_bytes);
         CUtensorMap omap;
         std::memset(&omap, 0, sizeof(omap));
         const int map_ok = out_type == FCWT_OUT_C64
