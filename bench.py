@@ -840,8 +840,8 @@ def run_sharded(args, world: int, rank: int, local_rank: int) -> None:
         "roofline": {"bound": "hbm", "achieved": algo0 / (k0 / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": algo0 / (k0 / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
                      "kernel": "k_row_tc (rank 0 block)", "kernel_ms": k0, "algorithmic_bytes": algo0},
-        "gather": {"ms": gather_ms, "bytes": 8 * points, "what": "NCCL gather of all row blocks to rank 0 "
-                                                                  "(float32 pairs, blocks padded to the largest)"},
+        "gather": {"ms": gather_ms, "bytes": 8 * points, "what": "row blocks sent point to point (NCCL) "
+                                                                  "into their rows of one [fn, n] tensor on rank 0"},
         "e2e": {"value": points * e2e_steps / te, "unit": "points/s", "h2d_bytes_per_step": 4 * N_SAMPLES,
                 "d2h_bytes_per_step": 8 * points, "ms_per_step": 1e3 * te / e2e_steps,
                 "host_buffers": "pinned; each rank copies its row block to host"},

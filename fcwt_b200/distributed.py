@@ -110,23 +110,30 @@ class ShardedCWT:
         return out
 
     def gather(self, local, dst: int = 0):
-        """Full [fn, n] output on rank dst (None elsewhere). Shards are padded
-        to the largest block for the collective."""
+        """Full [fn, n] output on rank dst (None elsewhere). Each rank's block
+        travels point to point straight into its rows of the destination
+        tensor: no padding to the largest block and no second copy on dst.
+        Complex blocks travel as float32 pairs (backends without complex
+        support)."""
         import torch
 
-        maxr = max(e - b for b, e in self.blocks)
-        # complex tensors travel as float32 pairs (backends without complex support)
-        pad = torch.zeros((maxr, self.n, 2), dtype=torch.float32, device=local.device)
-        if local.shape[0]:
-            pad[: local.shape[0]] = torch.view_as_real(local)
-        parts = [torch.empty_like(pad) for _ in range(self.world)] if self.rank == dst else None
-        self.dist.gather(pad, gather_list=parts, dst=dst, group=self.group)
         if self.rank != dst:
+            if local.shape[0]:
+                self.dist.send(torch.view_as_real(local.contiguous()), dst=dst, group=self.group)
             return None
-        full = torch.empty((self.fn, self.n, 2), dtype=torch.float32, device=local.device)
-        for (b, e), p in zip(self.blocks, parts):
-            full[b:e] = p[: e - b]
-        return torch.view_as_complex(full)
+        full = torch.empty((self.fn, self.n), dtype=torch.complex64, device=local.device)
+        fr = torch.view_as_real(full)
+        reqs = []
+        for r, (b, e) in enumerate(self.blocks):
+            if e == b:
+                continue
+            if r == self.rank:
+                fr[b:e].copy_(torch.view_as_real(local))
+            else:
+                reqs.append(self.dist.irecv(fr[b:e], src=r, group=self.group))
+        for q in reqs:
+            q.wait()
+        return full
 
     def close(self):
         if self.plan is not None:
