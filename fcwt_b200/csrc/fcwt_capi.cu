@@ -142,13 +142,6 @@ int check_pointer_devices(std::initializer_list<const void*> ptrs, int dev) {
     return FCWT_OK;
 }
 
-// Kernel variant switch read from the environment (0/1), `def` when unset.
-int tc_variant(const char* name, int def) {
-    const char* v = std::getenv(name);
-    if (!v || !v[0]) return def;
-    return v[0] != '0' ? 1 : 0;
-}
-
 size_t out_elem_bytes(int out_type) { return out_type == FCWT_OUT_C64 ? 8 : 4; }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -752,8 +745,7 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
         for (int s = 0; s < nsig; s++) tp.outs[s] = dout[s];
         tp.err = ep.err;
         tp.tma_store = map_ok;
-        tp.c64_dft = tc_variant("FCWT_TC_C64_DFT", 0);
-        tp.direct16 = tc_variant("FCWT_TC_DIRECT16", 0);
+        tp.decimated = P->sig.size() == 1 && P->sig[0].dec > 1;
         FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_tc, ctx->num_sms)), st));
         ctx->kernel_launches += 1;
     }
@@ -840,8 +832,7 @@ int run_pipelined(fcwt_plan* P, const void* din, void* hout, int out_type) {
         tp.outs[0] = base;
         tp.err = ctx->err.as<int>();
         tp.tma_store = map_ok;
-        tp.c64_dft = tc_variant("FCWT_TC_C64_DFT", 0);
-        tp.direct16 = tc_variant("FCWT_TC_DIRECT16", 0);
+        tp.decimated = P->sig.size() == 1 && P->sig[0].dec > 1;
         FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(r1 - r0, ctx->num_sms)), st));
         ctx->kernel_launches += 1;
         FCWT_CUDA_TRY(cudaEventRecord(ctx->pipe_done[slot], st));

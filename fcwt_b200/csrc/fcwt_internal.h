@@ -131,8 +131,7 @@ struct TcParams {
     void* outs[kMaxOuts];
     int* err;
     int tma_store;             // outputs via the tensor map (buffer 0, complex64, even n)
-    int c64_dft;               // complex64 rows: column DFTs as split-FP16 tensor-core stages
-    int direct16;              // 16-bit outputs: stores straight from the stage-2 results (no staging)
+    int decimated;             // some row has RowDesc::dec > 1 (selects the decimating kernel)
 };
 
 // Error bits written by device code into EngineParams::err.

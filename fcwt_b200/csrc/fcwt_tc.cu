@@ -35,6 +35,8 @@
 //             as well (two radix-32 GEMM stages, row_tc_dft).
 // Tensor memory: 512 columns per CTA (A: 0..255, accumulators of half h:
 // 256 + 128 h + 16 t for tile t).
+#include <initializer_list>
+
 #include "fcwt_dev.cuh"
 
 namespace fcwt {
@@ -54,8 +56,7 @@ constexpr int kTcBBytes = 16 * 2 * kTcMaxKp * 2;  // one B operand (16 rows x 2K
 constexpr int kTcOffTg = kTcOffB + 2 * 2 * kTcBBytes;
 constexpr int kTcOffW32 = (kTcOffTg + 2 * 32 * 8 + 1023) & ~1023;  // DFT-32 matrix, 128B-swizzled
 constexpr int kTcW32Bytes = 64 * 128;
-constexpr int kTcOffW32lo = kTcOffW32 + kTcW32Bytes;  // low FP16 part of W / 32 (complex64 DFT stages)
-constexpr int kTcOffEnd = kTcOffW32lo + kTcW32Bytes;
+constexpr int kTcOffEnd = kTcOffW32 + kTcW32Bytes;
 constexpr size_t kTcSmemBytes = (size_t)kTcOffEnd + 1024;
 constexpr int kTcStageBlock = 128 * 128;  // one 128-row block of a DFT-stage operand (16 KB)
 static_assert(4 * kBoxBytes == kTcGbufBytes, "staging boxes fill one G buffer");
@@ -287,7 +288,7 @@ __device__ __forceinline__ void tc_claim_next(const TcParams& P, int* next_idx, 
     }
 }
 
-template <int KP, int OT>
+template <int KP, int OT, bool DEC>
 __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                        const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                        const float2* __restrict__ twhi, const float2* __restrict__ t2, uint32_t tmem,
@@ -304,7 +305,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int N = 1 << log2N;
     const int M = N >> kLog2P2;
     const unsigned Nm = (unsigned)N - 1u;
-    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
+    const int D = DEC ? R.dec : 1;  // time decimation: column c = D c', output sample t' = c' + Mo a
     const int Mo = M / D;
     const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
@@ -350,7 +351,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
             tmem_wait_ld();
             const int k2 = lane + 32 * (8 * qd + tb + tt);
             float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], inv));
-            const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
+            const float2 stp = DEC ? tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm) : twlo[k2];
 #pragma unroll
             for (int j = 0; j < kTcCols; j++) {
                 gv[tt][j] = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
@@ -461,211 +462,7 @@ __device__ __forceinline__ void issue_dft_stage(uint32_t d, uint32_t a, uint32_t
                    umma_desc_sw128(w + 32u * kb), kTcIdescDft, kb != 0 ? 1u : 0u);
 }
 
-// The same stage in split FP16: D = A_hi W_hi + A_lo W_hi + A_hi W_lo (about
-// 2^-22 relative per product), for complex64 outputs.
-__device__ __forceinline__ void issue_dft_stage_split(uint32_t d, uint32_t ahi, uint32_t alo, uint32_t whi,
-                                                      uint32_t wlo) {
-    // opaque copies: keeps the compiler from hoisting the 24 descriptors out of
-    // the group loop (48 registers held by every thread of the CTA)
-    asm volatile("" : "+r"(ahi), "+r"(alo), "+r"(whi), "+r"(wlo));
-#pragma unroll
-    for (int m = 0; m < 2; m++)
-#pragma unroll
-        for (int kb = 0; kb < 4; kb++) {
-            const uint32_t ao = (uint32_t)(kTcStageBlock * m) + 32u * kb;
-            mma_ss(d + 64u * m, umma_desc_sw128(ahi + ao), umma_desc_sw128(whi + 32u * kb), kTcIdescDft,
-                   kb != 0 ? 1u : 0u);
-            mma_ss(d + 64u * m, umma_desc_sw128(alo + ao), umma_desc_sw128(whi + 32u * kb), kTcIdescDft, 1u);
-            mma_ss(d + 64u * m, umma_desc_sw128(ahi + ao), umma_desc_sw128(wlo + 32u * kb), kTcIdescDft, 1u);
-        }
-}
-
-__device__ __forceinline__ void split_h2(float2 v, uint32_t& hi, uint32_t& lo) {
-    const __half2 h = __floats2half2_rn(v.x, v.y);
-    const float2 f = __half22float2(h);
-    hi = h2bits(h);
-    lo = h2bits(__floats2half2_rn(v.x - f.x, v.y - f.y));
-}
-
-// Complex64 rows with the column DFTs on the tensor cores: the two radix-32
-// stages of row_tc_dft below, in split FP16 (three products per stage, both
-// operands hi + lo), after a split-FP16 phase 1. The stage-2 accumulators of
-// a warp are [4 a][8 c] tiles of the output, i.e. four 64-byte runs of 8
-// consecutive samples, so each thread stores its 32 results straight to the
-// output (coalesced, streaming) and no staging buffer is needed: the half's
-// 64 KB region holds the stage operand's hi (first 32 KB) and lo parts.
-template <int KP>
-__device__ __forceinline__ void row_tc_c64dft(const TcParams& P, const RowDesc& R, const SigDesc& S,
-                                              unsigned char* sm, const float2* __restrict__ twlo,
-                                              const float2* __restrict__ twhi, const float2* __restrict__ t2,
-                                              uint32_t tmem, uint32_t mbar_h, uint32_t& phase, uint32_t mbar2_h,
-                                              uint32_t& phase2, float* s_red, int* next_idx, RowDesc* next_R,
-                                              SigDesc* next_S) {
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int h = warp >> 3;
-    const int ht = tid & 255;
-    const int wl = warp & 7;
-    const int qd = warp & 3;
-    const int log2N = S.log2N;
-    const int N = 1 << log2N;
-    const int M = N >> kLog2P2;
-    const unsigned Nm = (unsigned)N - 1u;
-    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
-    const int Mo = M / D;
-    const int n = R.n_out;     // output samples of the row
-    const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
-
-    const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
-    const float s1 = 1.0f / (float)KP;
-    const float fin = inv * (float)(KP * 1024);
-
-    const int ng = Mo / kTcCols;
-    unsigned char* ahi = sm + h * kTcGbufBytes;  // stage operand, high parts (32 KB)
-    unsigned char* alo = ahi + kTcGbufBytes / 2; // stage operand, low parts (32 KB)
-    unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
-    unsigned char* blo = bhi + kTcBBytes;
-    float2* tg = reinterpret_cast<float2*>(sm + kTcOffTg) + 32 * h;
-    const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
-    const uint32_t ahi_a = smem_u32(ahi), alo_a = smem_u32(alo);
-    const uint32_t whi_a = smem_u32(sm + kTcOffW32), wlo_a = smem_u32(sm + kTcOffW32lo);
-    const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
-    float2* outb = reinterpret_cast<float2*>(P.outs[R.out_buf]);
-    int g = h;
-    if (g < ng) {
-        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
-        fence_proxy_async_smem();
-        half_bar(h);
-        if (lane == 0) {
-            tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
-            mma_commit(mbar_h);
-        }
-    }
-    const int tb = (wl >> 2) * 4;
-    const int amax = (n + Mo - 1) / Mo;
-    const uint32_t a1_off = (uint32_t)((lane >> 3) * 1024 + (lane & 7) * 128 + ((((2 * qd + (tb >> 2)) ^ lane) & 7) << 4));
-    const uint32_t a2_off = (uint32_t)(wl * 128 + ((((lane >> 2) ^ wl) & 7) << 4) + (lane & 3) * 4);
-    const int my_a1 = 16 * (wl >> 2) + 4 * qd + (lane >> 3);
-    const int my_c = lane & 7;
-    const uint32_t dsrc = dcol + lane_base + 64u * (uint32_t)(wl >> 2);
-    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
-    while (g < ng) {
-        mbar_wait(mbar_h, phase, P.err);
-        phase ^= 1u;
-        tc_fence_after();
-        const int c0 = g * kTcCols;  // first output column c' of the group (column D c0 of the row)
-        // two tiles at a time: each thread's 16-byte piece of a row holds kb = 8 qd + tb + 0..3,
-        // written as two 8-byte halves (tt = 0, 1 and tt = 2, 3)
-#pragma unroll
-        for (int p = 0; p < 2; p++) {
-            uint32_t ph[kTcCols][2], pl[kTcCols][2];
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int tt = 2 * p + u;
-                uint32_t r[16];
-                tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
-                tmem_wait_ld();
-                const int k2 = lane + 32 * (8 * qd + tb + tt);
-                float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], s1));
-                const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
-#pragma unroll
-                for (int j = 0; j < kTcCols; j++) {
-                    split_h2(cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w), ph[j][u],
-                             pl[j][u]);
-                    if (j + 1 < kTcCols) w = cmul(w, stp);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < kTcCols; j++) {
-                const uint32_t o = (uint32_t)((j >> 2) * kTcStageBlock + (j & 3) * 4096 + 8 * p) + a1_off;
-                *reinterpret_cast<uint2*>(ahi + o) = make_uint2(ph[j][0], ph[j][1]);
-                *reinterpret_cast<uint2*>(alo + o) = make_uint2(pl[j][0], pl[j][1]);
-            }
-        }
-        tc_fence_before();
-        fence_proxy_async_smem();
-        half_bar(h);  // phase-1 accumulators drained; stage-1 operand in SMEM
-        if (wl == 0 && lane == 0) {
-            tc_fence_after();
-            issue_dft_stage_split(dcol, ahi_a, alo_a, whi_a, wlo_a);
-            mma_commit(mbar2_h);
-        }
-        const int gn = g + 2;
-        if (gn < ng) {
-            build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
-            fence_proxy_async_smem();
-        }
-        mbar_wait(mbar2_h, phase2, P.err);
-        phase2 ^= 1u;
-        tc_fence_after();
-#pragma unroll
-        for (int q4 = 0; q4 < 4; q4++) {
-            uint32_t r[16];
-            tmem_ld16(dsrc + 16u * q4, r);
-            tmem_wait_ld();
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int a1 = 8 * q4 + i;
-                const float2 v = cmul(make_float2(__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])),
-                                      t2[a1 * 32 + lane]);
-                uint32_t vh, vl;
-                split_h2(v, vh, vl);
-                const uint32_t o = (uint32_t)((a1 >> 4) * kTcStageBlock + (a1 & 15) * 1024) + a2_off;
-                *reinterpret_cast<uint32_t*>(ahi + o) = vh;
-                *reinterpret_cast<uint32_t*>(alo + o) = vl;
-            }
-        }
-        tc_fence_before();
-        fence_proxy_async_smem();
-        half_bar(h);  // stage-1 accumulators drained; stage-2 operand in SMEM
-        if (wl == 0 && lane == 0) {
-            tc_fence_after();
-            issue_dft_stage_split(dcol, ahi_a, alo_a, whi_a, wlo_a);
-            mma_commit(mbar2_h);
-        }
-        mbar_wait(mbar2_h, phase2, P.err);
-        phase2 ^= 1u;
-        tc_fence_after();
-        // sample t = c0 + my_c + M (my_a1 + 32 a2): per store instruction a warp
-        // writes four runs of 8 consecutive samples (64 bytes each). The first
-        // 16 a2 are stored before the barrier, the rest after the next MMAs issue.
-        const int c = c0 + my_c;
-        float2* orow = outb + R.out_off + c;
-        uint32_t r[32];
-        tmem_ld16(dsrc, *reinterpret_cast<uint32_t(*)[16]>(r));
-        tmem_ld16(dsrc + 16u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int a = my_a1 + 32 * i;
-            if (a < amax && c + (long long)Mo * a < n)
-                __stcs(orow + (long long)Mo * a,
-                       make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
-        }
-        tmem_ld16(dsrc + 32u, *reinterpret_cast<uint32_t(*)[16]>(r));
-        tmem_ld16(dsrc + 48u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
-        tmem_wait_ld();
-        tc_fence_before();
-        half_bar(h);  // accumulators and the stage operand free for the next group
-        if (lane == 0 && gn < ng) {
-            tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
-            mma_commit(mbar_h);
-        }
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int a = my_a1 + 32 * (16 + i);
-            if (a < amax && c + (long long)Mo * a < n)
-                __stcs(orow + (long long)Mo * a,
-                       make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
-        }
-        g = gn;
-    }
-}
-
-template <int KP, int OT>
+template <int KP, int OT, bool DEC>
 __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                            const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                            const float2* __restrict__ twhi, const float2* __restrict__ t2,
@@ -683,7 +480,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const int N = 1 << log2N;
     const int M = N >> kLog2P2;
     const unsigned Nm = (unsigned)N - 1u;
-    const int D = R.dec;       // time decimation: column c = D c', output sample t' = c' + Mo a
+    const int D = DEC ? R.dec : 1;  // time decimation: column c = D c', output sample t' = c' + Mo a
     const int Mo = M / D;
     const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
@@ -740,7 +537,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
                 tmem_wait_ld();
                 const int k2 = lane + 32 * (8 * qd + tb + tt);
                 float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], s1));
-                const float2 stp = D == 1 ? twlo[k2] : tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm);
+                const float2 stp = DEC ? tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm) : twlo[k2];
 #pragma unroll
                 for (int j = 0; j < kTcCols; j++) {
                     const float2 v = cmul(make_float2(__uint_as_float(r[j]), __uint_as_float(r[8 + j])), w);
@@ -809,24 +606,12 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
                     make_float2(__uint_as_float(r[2 * i]) * fin, __uint_as_float(r[2 * i + 1]) * fin));
         }
         tc_fence_before();
-        if (tma && !P.direct16 && lane == 0 && wl >= 4) bulk_wait_read_all();
+        if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators free for the next group; staging free
         if (lane == 0 && gn < ng) {
             tc_fence_after();
             issue_group<KP, false>(wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
-        }
-        if (P.direct16) {
-            // straight to the output: four 32-byte runs of 8 samples per store instruction
-            const int c = c0 + my_c;
-            unsigned* orow = reinterpret_cast<unsigned*>(outb) + R.out_off + c;
-#pragma unroll
-            for (int a2 = 0; a2 < 32; a2++) {
-                const int a = my_a1 + 32 * a2;
-                if (a < amax && c + (long long)Mo * a < n) __stcs(orow + (long long)Mo * a, yv[a2]);
-            }
-            g = gn;
-            continue;
         }
         // a = my_a1 + 32 a2 with my_a1 < 32: box a2 / 8, box row my_a1 + 32 (a2 % 8), same swizzle bit
 #pragma unroll
@@ -866,8 +651,9 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     }
 }
 
-// TDFT: complex64 rows with the column DFTs on the tensor cores (row_tc_c64dft).
-template <int OT, bool TDFT = false>
+// DEC: the launch holds time-decimated rows (RowDesc::dec > 1); without it the
+// decimation arithmetic is compiled out.
+template <int OT, bool DEC = false>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_row_tc(const __grid_constant__ TcParams P, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
@@ -893,20 +679,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         sincospi(2.0 * (double)((a * l) & 1023) / 1024.0, &s, &c);
         t2[j] = make_float2((float)c, (float)s);
     }
-    if (OT == OUT_BF16 || OT == OUT_F16 || TDFT) {
-        // W / 32 for the DFT stages: row n = 2 a + {re, im}, K index 2 k + {re, im};
-        // high FP16 part at kTcOffW32, low part (value - high) at kTcOffW32lo
+    if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
+        // W / 32 for the DFT stages: row n = 2 a + {re, im}, K index 2 k + {re, im}
         unsigned char* w32 = sm + kTcOffW32;
-        unsigned char* w32lo = sm + kTcOffW32lo;
         for (int j = tid; j < 64 * 64; j += kTcThreads) {
             const int nr = j >> 6, k = j & 63;
             double s, c;
             sincospi((double)(((nr >> 1) * (k >> 1)) & 31) / 16.0, &s, &c);
             const float cv = (float)c * (1.0f / 32.0f), sv = (float)s * (1.0f / 32.0f);
             const float v = (nr & 1) == 0 ? ((k & 1) == 0 ? cv : -sv) : ((k & 1) == 0 ? sv : cv);
-            const __half hv = __float2half_rn(v);
-            *reinterpret_cast<__half*>(w32 + sw128_off(nr, 2 * k)) = hv;
-            *reinterpret_cast<__half*>(w32lo + sw128_off(nr, 2 * k)) = __float2half_rn(v - __half2float(hv));
+            *reinterpret_cast<__half*>(w32 + sw128_off(nr, 2 * k)) = __float2half_rn(v);
         }
         fence_proxy_async_smem();
     }
@@ -957,24 +739,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const float2* twhi = M <= kTcTwhiSmem ? twhi_s : S.tw + kP2;
         if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
             if (R.kp > 8)
-                row_tc_dft<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
+                row_tc_dft<16, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
                                    &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
             else
-                row_tc_dft<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
+                row_tc_dft<8, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
                                   &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
-        } else if constexpr (TDFT) {
-            if (R.kp > 8)
-                row_tc_c64dft<16>(P, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
-                                  &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
-            else
-                row_tc_c64dft<8>(P, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
-                                 &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
         } else {
             if (R.kp > 8)
-                row_tc<16, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                row_tc<16, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
                                &s_R[sl ^ 1], &s_S[sl ^ 1]);
             else
-                row_tc<8, OT>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                row_tc<8, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
                               &s_R[sl ^ 1], &s_S[sl ^ 1]);
         }
         tc_fence_before();
@@ -1017,39 +792,39 @@ cudaError_t launch_tc_weights(const SigDesc* sigs, const RowDesc* rows, const in
 
 size_t tc_smem_bytes() { return dev::kTcSmemBytes; }
 
-cudaError_t tc_configure() {
-    cudaError_t e = cudaFuncSetAttribute(dev::k_row_tc<OUT_C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)dev::kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_C64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dev::kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dev::kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dev::kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(dev::k_row_tc<OUT_POWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dev::kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(dev::k_row_tc<OUT_DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int OT, bool DEC>
+cudaError_t tc_configure_one() {
+    return cudaFuncSetAttribute(dev::k_row_tc<OT, DEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dev::kTcSmemBytes);
 }
 
-cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st) {
+cudaError_t tc_configure() {
+    cudaError_t e = cudaSuccess;
+    for (cudaError_t r : {tc_configure_one<OUT_C64, false>(), tc_configure_one<OUT_C64, true>(),
+                          tc_configure_one<OUT_BF16, false>(), tc_configure_one<OUT_BF16, true>(),
+                          tc_configure_one<OUT_F16, false>(), tc_configure_one<OUT_F16, true>(),
+                          tc_configure_one<OUT_POWER, false>(), tc_configure_one<OUT_POWER, true>(),
+                          tc_configure_one<OUT_DB, false>(), tc_configure_one<OUT_DB, true>()})
+        if (r != cudaSuccess && e == cudaSuccess) e = r;
+    return e;
+}
+
+template <bool DEC>
+void launch_tc_dec(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st) {
     switch (out_type) {
-        case OUT_BF16: dev::k_row_tc<OUT_BF16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
-        case OUT_F16: dev::k_row_tc<OUT_F16><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
-        case OUT_POWER: dev::k_row_tc<OUT_POWER><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
-        case OUT_DB: dev::k_row_tc<OUT_DB><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
-        default:
-            if (p.c64_dft)
-                dev::k_row_tc<OUT_C64, true><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap);
-            else
-                dev::k_row_tc<OUT_C64><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap);
-            break;
+        case OUT_BF16: dev::k_row_tc<OUT_BF16, DEC><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_F16: dev::k_row_tc<OUT_F16, DEC><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_POWER: dev::k_row_tc<OUT_POWER, DEC><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        case OUT_DB: dev::k_row_tc<OUT_DB, DEC><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
+        default: dev::k_row_tc<OUT_C64, DEC><<<grid, dev::kTcThreads, dev::kTcSmemBytes, st>>>(p, omap); break;
     }
+}
+
+cudaError_t launch_tc(const TcParams& p, const CUtensorMap& omap, int out_type, int grid, cudaStream_t st) {
+    if (p.decimated)
+        launch_tc_dec<true>(p, omap, out_type, grid, st);
+    else
+        launch_tc_dec<false>(p, omap, out_type, grid, st);
     return cudaGetLastError();
 }
 
