@@ -201,6 +201,27 @@ __device__ __forceinline__ void issue_group(int t, uint32_t tmem, uint32_t dcol,
     }
 }
 
+// Runtime switch between the two window widths (8 or 16 blocks): only the
+// B operand, the MMA issue and the pre-pass depend on it, so the group loop
+// of a row is compiled once (half the instruction footprint of the hot loop).
+template <bool LO>
+__device__ __forceinline__ void build_b_kp(bool kp16, float2* __restrict__ tg, int g, int ht, int M, unsigned Nm,
+                                           int L, const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                                           unsigned char* bhi, unsigned char* blo, int D) {
+    if (kp16)
+        build_b<16, LO>(tg, g, ht, M, Nm, L, twlo, twhi, bhi, blo, D);
+    else
+        build_b<8, LO>(tg, g, ht, M, Nm, L, twlo, twhi, bhi, blo, D);
+}
+template <bool LO>
+__device__ __forceinline__ void issue_group_kp(bool kp16, int t, uint32_t tmem, uint32_t dcol, uint32_t bhi,
+                                               uint32_t blo) {
+    if (kp16)
+        issue_group<16, LO>(t, tmem, dcol, bhi, blo);
+    else
+        issue_group<8, LO>(t, tmem, dcol, bhi, blo);
+}
+
 // Pre-pass of a row: Z on the window, scaled by 2^e (max |Z| 2^e in
 // [2^14, 2^15)) and split into FP16 hi + lo, into tensor memory as the A
 // operand (tile t, lane 32 q + l holds k2 = l + 32 (8 q + t)). Returns 2^-e.
@@ -288,12 +309,12 @@ __device__ __forceinline__ void tc_claim_next(const TcParams& P, int* next_idx, 
     }
 }
 
-template <int KP, int OT, bool DEC>
+template <int OT, bool DEC>
 __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                        const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                        const float2* __restrict__ twhi, const float2* __restrict__ t2, uint32_t tmem,
                                        uint32_t mbar_h, uint32_t& phase, float* s_red, int* next_idx,
-                                       RowDesc* next_R, SigDesc* next_S) {
+                                       RowDesc* next_R, SigDesc* next_S, bool kp16) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -310,7 +331,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
-    const float inv = tc_prepass<KP>(P, R, S, tmem, s_red);
+    const float inv = (kp16 ? tc_prepass<16>(P, R, S, tmem, s_red) : tc_prepass<8>(P, R, S, tmem, s_red));
 
     // ---- column groups
     const int ng = Mo / kTcCols;
@@ -324,12 +345,12 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
+        build_b_kp<true>(kp16, tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
             tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group_kp<true>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
     }
@@ -362,7 +383,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators drained; the G buffer is free
         const int gn = g + 2;
-        if (gn < ng) build_b<KP>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
+        if (gn < ng) build_b_kp<true>(kp16, tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
             const int k2 = lane + 32 * (8 * qd + tb + tt);
@@ -373,7 +394,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         half_bar(h);  // G tiles and the next B in SMEM
         if (lane == 0 && gn < ng) {
             tc_fence_after();
-            issue_group<KP>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group_kp<true>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
         // phase 2: one column per warp
@@ -462,13 +483,13 @@ __device__ __forceinline__ void issue_dft_stage(uint32_t d, uint32_t a, uint32_t
                    umma_desc_sw128(w + 32u * kb), kTcIdescDft, kb != 0 ? 1u : 0u);
 }
 
-template <int KP, int OT, bool DEC>
+template <int OT, bool DEC>
 __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap* omap, const RowDesc& R,
                                            const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                            const float2* __restrict__ twhi, const float2* __restrict__ t2,
                                            uint32_t tmem, uint32_t mbar_h, uint32_t& phase, uint32_t mbar2_h,
                                            uint32_t& phase2, float* s_red, int* next_idx, RowDesc* next_R,
-                                           SigDesc* next_S) {
+                                           SigDesc* next_S, bool kp16) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -485,9 +506,9 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const int n = R.n_out;     // output samples of the row
     const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
 
-    const float inv = tc_prepass<KP, false>(P, R, S, tmem, s_red);
-    const float s1 = 1.0f / (float)KP;
-    const float fin = inv * (float)(KP * 1024);
+    const float inv = (kp16 ? tc_prepass<16, false>(P, R, S, tmem, s_red) : tc_prepass<8, false>(P, R, S, tmem, s_red));
+    const float s1 = kp16 ? 1.0f / 16.0f : 1.0f / 8.0f;
+    const float fin = inv * (float)((kp16 ? 16 : 8) * 1024);
 
     const int ng = Mo / kTcCols;
     unsigned char* abuf = sm + h * kTcGbufBytes;        // DFT-stage A operand, 32 KB
@@ -502,12 +523,12 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
-        build_b<KP, false>(tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
+        build_b_kp<false>(kp16, tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
         if (lane == 0) {
             tc_fence_after();
-            issue_group<KP, false>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group_kp<false>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
     }
@@ -560,7 +581,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         }
         const int gn = g + 2;
         if (gn < ng) {
-            build_b<KP, false>(tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
+            build_b_kp<false>(kp16, tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
             fence_proxy_async_smem();
         }
         mbar_wait(mbar2_h, phase2, P.err);
@@ -610,7 +631,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         half_bar(h);  // accumulators free for the next group; staging free
         if (lane == 0 && gn < ng) {
             tc_fence_after();
-            issue_group<KP, false>(wl, tmem, dcol, bhi_a, blo_a);
+            issue_group_kp<false>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
         }
         // a = my_a1 + 32 a2 with my_a1 < 32: box a2 / 8, box row my_a1 + 32 (a2 % 8), same swizzle bit
@@ -738,19 +759,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (tid == 0) s_log2N = log2N;
         const float2* twhi = M <= kTcTwhiSmem ? twhi_s : S.tw + kP2;
         if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
-            if (R.kp > 8)
-                row_tc_dft<16, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
-                                   &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
-            else
-                row_tc_dft<8, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
-                                  &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1]);
+            row_tc_dft<OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
+                                &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1], R.kp > 8);
         } else {
-            if (R.kp > 8)
-                row_tc<16, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
-                               &s_R[sl ^ 1], &s_S[sl ^ 1]);
-            else
-                row_tc<8, OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
-                              &s_R[sl ^ 1], &s_S[sl ^ 1]);
+            row_tc<OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
+                            &s_R[sl ^ 1], &s_S[sl ^ 1], R.kp > 8);
         }
         tc_fence_before();
         __syncthreads();
