@@ -59,7 +59,7 @@ THREADS = os.cpu_count() or 1
 # output type, from one-pass ncu captures of the full-size launch
 # (dram__bytes_read.sum + dram__bytes_write.sum; the capture summaries are
 # kept under profiles/, named for the kernel and the workload)
-TRAFFIC_PER_LAUNCH = {"complex64": 147.76e6 + 2.3459e9, "bf16": 152.88e6 + 1.1459e9}
+TRAFFIC_PER_LAUNCH = {"complex64": 147.96e6 + 2.34565e9, "bf16": 156.01e6 + 1.14550e9}
 
 # --out choices: (constant in fcwt_b200, trailing shape, torch dtype, bytes per point)
 OUT_TYPES = {
