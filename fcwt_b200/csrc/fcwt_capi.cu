@@ -258,7 +258,20 @@ struct fcwt_plan {
     std::vector<PlanSignal> sig;
     std::vector<PlanTables> tables;
     DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs, tc_rows, tc_wts;
-    fcwt::FwdJob* jobs_host = nullptr;  // pinned staging of the batched forward jobs
+    // Per-execution uploads of batched plans (forward jobs, per-output tensor
+    // maps) go through a ring of pinned host slots; a slot is rewritten only
+    // after the copy that read it has run (its event), so back-to-back
+    // executions with different buffers never see each other's data.
+    struct UploadSlot {
+        void* host = nullptr;
+        size_t bytes = 0;
+        cudaEvent_t done = nullptr;
+        bool pending = false;
+    };
+    std::array<UploadSlot, 4> uploads;
+    int upload_next = 0;
+    DevBuf tmaps, graph_tmaps;               // per-output tensor maps (batched plans), device copies
+    std::array<unsigned long long, fcwt::kMaxOuts / 64> graph_tmap_mask{};
     int n_items = 0;
     int n_rows = 0;
     int n_tc = 0;  // rows run by the tensor-core engine
@@ -307,7 +320,13 @@ void plan_free(fcwt_plan* p) {
     p->sigs2.release();
     p->ds_tmp.release();
     p->shifted.release();
-    if (p->jobs_host) cudaFreeHost(p->jobs_host);
+    for (auto& u : p->uploads) {
+        if (u.pending && u.done) cudaEventSynchronize(u.done);
+        if (u.host) cudaFreeHost(u.host);
+        if (u.done) cudaEventDestroy(u.done);
+    }
+    p->tmaps.release();
+    p->graph_tmaps.release();
     delete p;
 }
 
@@ -503,7 +522,7 @@ int plan_build(fcwt_plan* P) {
     if (nsig > 1) {
         FCWT_CUDA_TRY(P->fwd_tmp.ensure(tmp_elems * sizeof(float2)));
         FCWT_CUDA_TRY(P->fwd_jobs.ensure((size_t)nsig * sizeof(FwdJob)));
-        FCWT_CUDA_TRY(cudaMallocHost(&P->jobs_host, (size_t)nsig * sizeof(FwdJob)));
+        FCWT_CUDA_TRY(P->tmaps.ensure((size_t)nsig * sizeof(CUtensorMap)));
     }
     FCWT_CUDA_TRY(P->pool.ensure(std::max<size_t>(pool.size(), 1) * sizeof(float)));
     FCWT_CUDA_TRY(P->sigs.ensure(sds.size() * sizeof(SigDesc)));
@@ -563,8 +582,42 @@ void job_groups(const fcwt_plan* P, std::vector<std::pair<int, int>>& groups) {
     }
 }
 
-// Fills P->jobs_host with the forward jobs of all signals ordered by table.
-void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int, int>>& groups) {
+// A pinned host buffer of at least `bytes` that no enqueued copy still reads.
+int upload_slot(fcwt_plan* P, size_t bytes, fcwt_plan::UploadSlot** out) {
+    fcwt_plan::UploadSlot& u = P->uploads[(size_t)P->upload_next];
+    P->upload_next = (P->upload_next + 1) % (int)P->uploads.size();
+    if (u.pending) FCWT_CUDA_TRY(cudaEventSynchronize(u.done));
+    u.pending = false;
+    if (!u.done) FCWT_CUDA_TRY(cudaEventCreateWithFlags(&u.done, cudaEventDisableTiming));
+    if (u.bytes < bytes) {
+        if (u.host) cudaFreeHost(u.host);
+        u.host = nullptr;
+        u.bytes = 0;
+        FCWT_CUDA_TRY(cudaMallocHost(&u.host, bytes));
+        u.bytes = bytes;
+    }
+    *out = &u;
+    return FCWT_OK;
+}
+
+// The tensor maps of every output of a batched plan (entry s for output s)
+// and the mask of the outputs whose map could be encoded.
+void build_output_maps(const fcwt_plan* P, void* const* dout, int out_type, CUtensorMap* maps,
+                       unsigned long long* mask) {
+    for (int i = 0; i < fcwt::kMaxOuts / 64; i++) mask[i] = 0;
+    for (size_t s = 0; s < P->sig.size(); s++) {
+        const PlanSignal& S = P->sig[s];
+        std::memset(&maps[s], 0, sizeof(CUtensorMap));
+        if (S.rows_out() == 0 || S.sp.N < fcwt::kTcMinN) continue;
+        const bool ok = out_type == FCWT_OUT_C64
+                            ? encode_output_map(dout[s], S.n_out(), S.sp.M / S.dec, S.rows_out(), &maps[s])
+                            : encode_output_map16(dout[s], S.n_out(), S.sp.M / S.dec, S.rows_out(), &maps[s]);
+        if (ok) mask[s >> 6] |= 1ull << (s & 63);
+    }
+}
+
+// Fills `jobs` with the forward jobs of all signals ordered by table.
+void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int, int>>& groups, fcwt::FwdJob* jobs) {
     using namespace fcwt;
     const int nsig = (int)P->sig.size();
     std::vector<size_t> tmp_off((size_t)nsig);
@@ -578,7 +631,7 @@ void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int,
         for (int s = 0; s < nsig; s++) {
             PlanSignal& S = P->sig[(size_t)s];
             if (S.table != (int)t) continue;
-            FwdJob& j = P->jobs_host[k++];
+            FwdJob& j = jobs[k++];
             j.in_r = S.sp.is_complex ? nullptr : (const float*)din[s];
             j.in_c = S.sp.is_complex ? (const float2*)din[s] : nullptr;
             j.n = S.sp.n;
@@ -590,12 +643,14 @@ void build_jobs(fcwt_plan* P, const void* const* din, std::vector<std::pair<int,
     job_groups(P, groups);
 }
 
-int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type);
+int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type,
+                 bool graph_maps = false);
 int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* graph_jobs);
 
 // Enqueues the forward FFTs and the row engine for device-resident inputs and
 // outputs (no host synchronisation, so it can be captured into a graph).
-// graph_jobs: device copy of the forward jobs prepared before a capture.
+// graph_jobs: device copy of the forward jobs prepared before a capture; the
+// per-output tensor maps of a batched plan are then plan->graph_tmaps.
 int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int out_type, bool allow_profiling,
                  const fcwt::FwdJob* graph_jobs = nullptr) {
     using namespace fcwt;
@@ -621,7 +676,7 @@ int plan_enqueue(fcwt_plan* P, const void* const* din, void* const* dout, int ou
         }
         FCWT_CUDA_TRY(cudaEventRecord(ev.first, st));
     }
-    rc = enqueue_rows(P, P->sigs.as<SigDesc>(), dout, out_type);
+    rc = enqueue_rows(P, P->sigs.as<SigDesc>(), dout, out_type, graph_jobs != nullptr);
     if (rc) return rc;
     if (P->doublesided) {
         // the mirrored half: exp(-2 pi i t / N) conj(V), V the rows on the shifted spectrum
@@ -674,9 +729,14 @@ int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* gr
         std::vector<std::pair<int, int>> groups;
         const FwdJob* djobs = graph_jobs;
         if (!djobs) {
-            build_jobs(P, din, groups);
-            FCWT_CUDA_TRY(cudaMemcpyAsync(P->fwd_jobs.p, P->jobs_host, (size_t)nsig * sizeof(FwdJob),
+            fcwt_plan::UploadSlot* u = nullptr;
+            int rc = upload_slot(P, (size_t)nsig * sizeof(FwdJob), &u);
+            if (rc) return rc;
+            build_jobs(P, din, groups, static_cast<FwdJob*>(u->host));
+            FCWT_CUDA_TRY(cudaMemcpyAsync(P->fwd_jobs.p, u->host, (size_t)nsig * sizeof(FwdJob),
                                           cudaMemcpyHostToDevice, st));
+            FCWT_CUDA_TRY(cudaEventRecord(u->done, st));
+            u->pending = true;
             djobs = P->fwd_jobs.as<FwdJob>();
         } else {
             job_groups(P, groups);
@@ -695,7 +755,7 @@ int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* gr
 
 // The row-engine launches of one pass over the plan's rows, reading the
 // spectra of `dsigs` and writing `dout`.
-int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type) {
+int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, int out_type, bool graph_maps) {
     using namespace fcwt;
     fcwt_context* ctx = P->ctx;
     cudaStream_t st = ctx->stream;
@@ -746,6 +806,24 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
         tp.err = ep.err;
         tp.tma_store = map_ok;
         tp.decimated = P->sig.size() == 1 && P->sig[0].dec > 1;
+        if (nsig > 1) {
+            // one tensor map per output, in device memory
+            if (graph_maps) {
+                tp.tmaps = P->graph_tmaps.as<CUtensorMap>();
+                for (int k = 0; k < kMaxOuts / 64; k++) tp.tmap_mask[k] = P->graph_tmap_mask[(size_t)k];
+            } else {
+                fcwt_plan::UploadSlot* u = nullptr;
+                int rc = upload_slot(P, (size_t)nsig * sizeof(CUtensorMap), &u);
+                if (rc) return rc;
+                build_output_maps(P, dout, out_type, static_cast<CUtensorMap*>(u->host), tp.tmap_mask);
+                FCWT_CUDA_TRY(cudaMemcpyAsync(P->tmaps.p, u->host, (size_t)nsig * sizeof(CUtensorMap),
+                                              cudaMemcpyHostToDevice, st));
+                FCWT_CUDA_TRY(cudaEventRecord(u->done, st));
+                u->pending = true;
+                tp.tmaps = P->tmaps.as<CUtensorMap>();
+            }
+            tp.tma_store = 1;
+        }
         FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_tc, ctx->num_sms)), st));
         ctx->kernel_launches += 1;
     }
@@ -1453,12 +1531,19 @@ int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* co
             FCWT_CUDA_TRY(ctx->scratch.ensure((size_t)plan->slots * (size_t)plan->slot_elems * sizeof(float2)));
         const fcwt::FwdJob* gj = nullptr;
         if (nsig > 1) {
+            // the graph reads its jobs and tensor maps from buffers of its own,
+            // filled once here (synchronously, before the capture)
             std::vector<std::pair<int, int>> groups;
-            build_jobs(plan, inputs, groups);
+            std::vector<fcwt::FwdJob> jobs((size_t)nsig);
+            build_jobs(plan, inputs, groups, jobs.data());
             FCWT_CUDA_TRY(plan->graph_jobs.ensure((size_t)nsig * sizeof(fcwt::FwdJob)));
-            FCWT_CUDA_TRY(cudaMemcpyAsync(plan->graph_jobs.p, plan->jobs_host, (size_t)nsig * sizeof(fcwt::FwdJob),
-                                          cudaMemcpyHostToDevice, st));
-            FCWT_CUDA_TRY(cudaStreamSynchronize(st));
+            FCWT_CUDA_TRY(cudaMemcpy(plan->graph_jobs.p, jobs.data(), (size_t)nsig * sizeof(fcwt::FwdJob),
+                                     cudaMemcpyHostToDevice));
+            std::vector<CUtensorMap> maps((size_t)nsig);
+            build_output_maps(plan, outputs, out_type, maps.data(), plan->graph_tmap_mask.data());
+            FCWT_CUDA_TRY(plan->graph_tmaps.ensure((size_t)nsig * sizeof(CUtensorMap)));
+            FCWT_CUDA_TRY(cudaMemcpy(plan->graph_tmaps.p, maps.data(), (size_t)nsig * sizeof(CUtensorMap),
+                                     cudaMemcpyHostToDevice));
             gj = plan->graph_jobs.as<fcwt::FwdJob>();
         }
         // capture on the context's own stream (the legacy default stream

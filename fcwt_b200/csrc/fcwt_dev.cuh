@@ -77,6 +77,12 @@ __device__ __forceinline__ void store_out(void* base, long long idx, float2 v) {
 }
 
 // ---- bulk-async (TMA) store helpers
+// Orders a tensor map that a host copy wrote into global memory before this
+// thread's TMA operations that use it (tensor-map proxy acquire, system scope).
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;"
+                 ::"l"(reinterpret_cast<unsigned long long>(map)) : "memory");
+}
 // EVICT_FIRST marks the written lines evict-first in L2 (the output is a
 // stream that is not read again by the kernel).
 template <bool EVICT_FIRST = false>

@@ -20,6 +20,7 @@
 
 #include <stdint.h>
 
+#include <cuda.h>
 #include <vector_types.h>
 
 namespace fcwt {
@@ -132,6 +133,10 @@ struct TcParams {
     int* err;
     int tma_store;             // outputs via the tensor map (buffer 0, complex64, even n)
     int decimated;             // some row has RowDesc::dec > 1 (selects the decimating kernel)
+    // many outputs (batched plans): one tensor map per output buffer in global
+    // memory, used where bit `out_buf` of tmap_mask is set
+    const CUtensorMap* tmaps;
+    unsigned long long tmap_mask[kMaxOuts / 64];
 };
 
 // Error bits written by device code into EngineParams::err.

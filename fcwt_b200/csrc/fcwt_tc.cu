@@ -341,7 +341,12 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     float2* tg = reinterpret_cast<float2*>(sm + kTcOffTg) + 32 * h;
     const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
     const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
-    const bool tma = P.tma_store != 0 && R.out_buf == 0;  // the map matches the output type
+    // the tensor map of this row's output buffer: the launch's map (buffer 0) or, for
+    // many outputs, the buffer's own map in global memory
+    const CUtensorMap* map = P.tmaps ? P.tmaps + R.out_buf : omap;
+    const bool tma = P.tma_store != 0 &&
+                     (P.tmaps ? ((P.tmap_mask[R.out_buf >> 6] >> (R.out_buf & 63)) & 1ull) != 0 : R.out_buf == 0);
+    if (P.tmaps && tma) tensormap_acquire(map);
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
@@ -426,7 +431,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
                 const int j = wl - 4;
                 // complex64 output lines evict-first in L2 (measured ~1% faster; slower for 4-byte types)
                 if (j * kBoxRows < n_full)
-                    tma_store_3d<OT == OUT_C64>(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
+                    tma_store_3d<OT == OUT_C64>(map, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
             const int tail = n - n_full * Mo;
@@ -519,7 +524,10 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const uint32_t bhi_a = smem_u32(bhi), blo_a = smem_u32(blo);
     const uint32_t abuf_a = smem_u32(abuf), w32_a = smem_u32(sm + kTcOffW32);
     const uint32_t dcol = tmem + (uint32_t)(kTcDcol + 128 * h);
-    const bool tma = P.tma_store != 0 && R.out_buf == 0;
+    const CUtensorMap* map = P.tmaps ? P.tmaps + R.out_buf : omap;
+    const bool tma = P.tma_store != 0 &&
+                     (P.tmaps ? ((P.tmap_mask[R.out_buf >> 6] >> (R.out_buf & 63)) & 1ull) != 0 : R.out_buf == 0);
+    if (P.tmaps && tma) tensormap_acquire(map);
     void* outb = P.outs[R.out_buf];
     int g = h;
     if (g < ng) {
@@ -647,7 +655,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             const int n_full = n / Mo;
             if (lane == 0 && wl >= 4) {
                 const int j = wl - 4;
-                if (j * kBoxRows < n_full) tma_store_3d(omap, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
+                if (j * kBoxRows < n_full) tma_store_3d(map, stage + j * box_bytes, c0, j * kBoxRows, R.out_row);
                 bulk_commit();
             }
             const int tail = n - n_full * Mo;

@@ -99,3 +99,59 @@ def test_graph_first_execution_of_a_larger_plan(fcwt, oracle):
     for a, b in zip(outs, ref):
         assert torch.equal(a, b)
     bp.close()
+
+
+def test_back_to_back_executions_into_different_buffers(fcwt, oracle):
+    """Consecutive executions enqueue their forward jobs and per-output tensor
+    maps from host staging without waiting on the device: each must keep its
+    own buffers (complex64 and BF16 outputs, no synchronisation in between)."""
+    import torch
+
+    lengths = [40000, 9000, 70000, 25000, 131072]
+    xs, scs = _channels(oracle, 4, lengths)
+    bp = fcwt.BatchPlan(lengths, scs, fb=6.0, threads=1)
+    sets = []
+    for k in range(6):
+        ins = [torch.from_numpy(x * (1.0 + k)).cuda() for x in xs]
+        outs = bp.outputs_like()
+        o16 = [torch.empty((fn, n, 2), dtype=torch.bfloat16, device="cuda") for fn, n in zip(bp.fns, bp.ns)]
+        sets.append((k, ins, outs, o16))
+    torch.cuda.synchronize()
+    for k, ins, outs, o16 in sets:
+        bp.execute(ins, outs)
+        bp.execute(ins, o16, out_type=fcwt.FCWT_OUT_BF16)
+    torch.cuda.synchronize()
+    base = bp.outputs_like()
+    bp.execute([torch.from_numpy(x).cuda() for x in xs], base)
+    torch.cuda.synchronize()
+    for k, ins, outs, o16 in sets:
+        for a, b, h in zip(outs, base, o16):
+            assert rel_l2(a.cpu().numpy(), (1.0 + k) * b.cpu().numpy()) < 1e-5
+            h64 = torch.complex(h[..., 0].double(), h[..., 1].double())
+            assert rel_l2(h64.cpu().numpy(), a.cpu().numpy()) < 3e-3
+    for c in (0, 4):
+        assert rel_l2(base[c].cpu().numpy(), oracle.cwt_fp64(xs[c], scs[c], 6.0, 1, True)) < 1e-5
+    bp.close()
+
+
+def test_output_without_tensor_map(fcwt, oracle):
+    """An output whose base is only 8-byte aligned cannot be a TMA target: its
+    rows take the plain store path while the other outputs keep theirs."""
+    import torch
+
+    lengths = [30000, 50000, 30000]
+    xs, scs = _channels(oracle, 5, lengths)
+    bp = fcwt.BatchPlan(lengths, scs, fb=6.0, threads=1)
+    ins = [torch.from_numpy(x).cuda() for x in xs]
+    ref = bp.outputs_like()
+    bp.execute(ins, ref)
+    fn1, n1 = bp.fns[1], bp.ns[1]
+    raw = torch.full((fn1 * n1 + 1,), float("nan"), dtype=torch.complex64, device="cuda")
+    odd = raw[1:].view(fn1, n1)
+    assert odd.data_ptr() % 16 == 8
+    outs = [torch.empty_like(ref[0]), odd, torch.empty_like(ref[2])]
+    bp.execute(ins, outs)
+    torch.cuda.synchronize()
+    for a, b in zip(outs, ref):
+        assert torch.equal(a, b)
+    bp.close()
