@@ -218,6 +218,9 @@ struct fcwt_context {
     };
     std::vector<CacheEntry> cache;
     unsigned long long use_clock = 0;
+    // every live plan created on this context (cached or caller-owned): destroying
+    // the context releases their device resources and detaches them
+    std::vector<fcwt_plan*> plans;
     // host-output pipeline: copy stream, per-slot "rows done" / "block copied" events
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t pipe_done[2] = {nullptr, nullptr}, pipe_copied[2] = {nullptr, nullptr};
@@ -299,9 +302,11 @@ int ctx_prepare(fcwt_context* ctx) {
     return FCWT_OK;
 }
 
-void plan_free(fcwt_plan* p) {
-    if (!p) return;
+// Releases the device and pinned resources of a plan; the plan stays valid as
+// an empty shell (idempotent).
+void plan_release(fcwt_plan* p) {
     if (p->graph) cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
     for (auto& s : p->sig) s.X.release();
     for (auto& t : p->tables) {
         t.mother.release();
@@ -324,9 +329,26 @@ void plan_free(fcwt_plan* p) {
         if (u.pending && u.done) cudaEventSynchronize(u.done);
         if (u.host) cudaFreeHost(u.host);
         if (u.done) cudaEventDestroy(u.done);
+        u = fcwt_plan::UploadSlot{};
     }
     p->tmaps.release();
     p->graph_tmaps.release();
+}
+
+fcwt_plan* plan_new(fcwt_context* ctx) {
+    fcwt_plan* P = new fcwt_plan();
+    P->ctx = ctx;
+    ctx->plans.push_back(P);
+    return P;
+}
+
+void plan_free(fcwt_plan* p) {
+    if (!p) return;
+    if (p->ctx) {
+        auto& v = p->ctx->plans;
+        v.erase(std::remove(v.begin(), v.end(), p), v.end());
+    }
+    plan_release(p);
     delete p;
 }
 
@@ -1121,6 +1143,13 @@ int fcwt_context_destroy(fcwt_context* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto& e : ctx->cache) plan_free(e.plan);
     ctx->cache.clear();
+    // plans the caller still holds: free their resources now, keep the handles
+    // valid (fcwt_plan_destroy on them only frees the handle)
+    for (fcwt_plan* p : ctx->plans) {
+        plan_release(p);
+        p->ctx = nullptr;
+    }
+    ctx->plans.clear();
     ctx->in_stage.release();
     ctx->out_stage.release();
     ctx->tmp.release();
@@ -1302,8 +1331,7 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
     if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
     if (row_begin < 0 || row_end > fn || row_begin > row_end)
         return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
-    fcwt_plan* P = new fcwt_plan();
-    P->ctx = ctx;
+    fcwt_plan* P = plan_new(ctx);
     P->fb = fb;
     P->is_complex = is_complex != 0;
     P->sig.resize(1);
@@ -1311,12 +1339,12 @@ int fcwt_plan_create(fcwt_context* ctx, int n, int is_complex, float fb, const f
     P->sig[0].re = row_end;
     P->compat_align = (flags & FCWT_COMPAT_ALIGN) != 0;
     if (P->compat_align && (row_begin != 0 || row_end != fn)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN applies to whole plans (all rows)");
     }
     std::string err;
     if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sig[0].sp, err)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_INVALID, err);
     }
     rc = plan_build(P);
@@ -1345,8 +1373,7 @@ int fcwt_plan_create_strided(fcwt_context* ctx, int n, int is_complex, float fb,
     if (fn > 0 && !scales) return fail(FCWT_ERR_INVALID, "null scales");
     if (row_begin < 0 || row_end > fn || row_begin > row_end)
         return fail(FCWT_ERR_INVALID, "row range outside [0, fn]");
-    fcwt_plan* P = new fcwt_plan();
-    P->ctx = ctx;
+    fcwt_plan* P = plan_new(ctx);
     P->fb = fb;
     P->is_complex = is_complex != 0;
     P->sig.resize(1);
@@ -1356,11 +1383,11 @@ int fcwt_plan_create_strided(fcwt_context* ctx, int n, int is_complex, float fb,
     P->sig[0].dec = time_stride;
     std::string err;
     if (fcwt::plan_signal(n, is_complex != 0, fb, scales, fn, threads, flags, P->sig[0].sp, err)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_INVALID, err);
     }
     if (time_stride > std::max(1, n)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_INVALID, "time_stride larger than the signal");
     }
     rc = plan_build(P);
@@ -1403,8 +1430,7 @@ int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const floa
     for (int i = 0; i < N; i++)
         if (!std::isfinite(mother[i])) return fail(FCWT_ERR_INVALID, "the mother table holds a non-finite value");
     if ((flags & FCWT_DOUBLESIDED) && N < 2) return fail(FCWT_ERR_INVALID, "doublesided wavelets need n >= 2");
-    fcwt_plan* P = new fcwt_plan();
-    P->ctx = ctx;
+    fcwt_plan* P = plan_new(ctx);
     P->fb = 1.0f;
     P->is_complex = is_complex != 0;
     P->custom_mother.assign(mother, mother + N);
@@ -1412,7 +1438,7 @@ int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const floa
     P->doublesided = (flags & FCWT_DOUBLESIDED) != 0;
     P->compat_align = (flags & FCWT_COMPAT_ALIGN) != 0;
     if (P->compat_align && (P->doublesided || row_begin != 0 || row_end != fn)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_UNSUPPORTED, "FCWT_COMPAT_ALIGN applies to whole plans of single-sided wavelets");
     }
     P->sig.resize(1);
@@ -1420,7 +1446,7 @@ int fcwt_plan_create_mother(fcwt_context* ctx, int n, int is_complex, const floa
     P->sig[0].re = row_end;
     std::string err;
     if (fcwt::plan_signal(n, is_complex != 0, 1.0f, scales, fn, threads, flags, P->sig[0].sp, err, mother)) {
-        delete P;
+        plan_free(P);
         return fail(FCWT_ERR_INVALID, err);
     }
     rc = plan_build(P);
@@ -1456,20 +1482,19 @@ int fcwt_plan_create_batched(fcwt_context* ctx, int nsig, const int* ns, int is_
     *out = nullptr;
     if (nsig < 1 || nsig > fcwt::kMaxOuts) return fail(FCWT_ERR_INVALID, "nsig must be in [1, 1024]");
     if (!ns || !scales || !fns) return fail(FCWT_ERR_INVALID, "null array argument");
-    fcwt_plan* P = new fcwt_plan();
-    P->ctx = ctx;
+    fcwt_plan* P = plan_new(ctx);
     P->fb = fb;
     P->is_complex = is_complex != 0;
     P->sig.resize((size_t)nsig);
     for (int s = 0; s < nsig; s++) {
         if (ns[s] < 0 || fns[s] < 0 || (fns[s] > 0 && !scales[s])) {
-            delete P;
+            plan_free(P);
             return fail(FCWT_ERR_INVALID, "bad size or scales of signal " + std::to_string(s));
         }
         std::string err;
         if (fcwt::plan_signal(ns[s], is_complex != 0, fb, scales[s], fns[s], threads, flags, P->sig[(size_t)s].sp,
                               err)) {
-            delete P;
+            plan_free(P);
             return fail(FCWT_ERR_INVALID, "signal " + std::to_string(s) + ": " + err);
         }
         P->sig[(size_t)s].rb = 0;
@@ -1488,17 +1513,20 @@ int fcwt_plan_create_batched(fcwt_context* ctx, int nsig, const int* ns, int is_
 
 int fcwt_plan_execute(fcwt_plan* plan, const void* input, void* output, int out_type) {
     if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (!plan->ctx) return fail(FCWT_ERR_INVALID, "the plan's context was destroyed");
     if (plan->sig.size() != 1) return fail(FCWT_ERR_INVALID, "batched plan: use fcwt_plan_execute_batched");
     return plan_run(plan, input, output, out_type);
 }
 
 int fcwt_plan_execute_batched(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type) {
     if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (!plan->ctx) return fail(FCWT_ERR_INVALID, "the plan's context was destroyed");
     return plan_run_multi(plan, inputs, outputs, out_type);
 }
 
 int fcwt_plan_execute_graph(fcwt_plan* plan, const void* const* inputs, void* const* outputs, int out_type) {
     if (!plan) return fail(FCWT_ERR_INVALID, "null plan");
+    if (!plan->ctx) return fail(FCWT_ERR_INVALID, "the plan's context was destroyed");
     fcwt_context* ctx = plan->ctx;
     int rc = ctx_prepare(ctx);
     if (rc) return rc;

@@ -155,3 +155,36 @@ def test_output_without_tensor_map(fcwt, oracle):
     for a, b in zip(outs, ref):
         assert torch.equal(a, b)
     bp.close()
+
+
+def test_context_destroyed_before_its_plans(fcwt, oracle):
+    """Destroying a context first (any order is possible when a garbage
+    collector finalises both) releases its plans' device resources and leaves
+    their handles valid: executing one reports an error, destroying it is safe."""
+    import ctypes
+
+    import torch
+
+    from fcwt_b200 import _lib
+
+    lengths = [30000, 9000]
+    xs, scs = _channels(oracle, 6, lengths)
+    lib = _lib.load()
+    ctx = _lib.Context(0)
+    nsig = len(lengths)
+    h = ctypes.c_void_p()
+    _lib.call("fcwt_plan_create_batched", ctx.handle, nsig, (ctypes.c_int * nsig)(*lengths), 0, ctypes.c_float(6.0),
+              (ctypes.c_void_p * nsig)(*[sc.ctypes.data for sc in scs]),
+              (ctypes.c_int * nsig)(*[sc.size for sc in scs]), 1, _lib.FCWT_NORM, ctypes.byref(h))
+    ins = [torch.from_numpy(x).cuda() for x in xs]
+    outs = [torch.empty((sc.size, n), dtype=torch.complex64, device="cuda") for sc, n in zip(scs, lengths)]
+    in_arr = (ctypes.c_void_p * nsig)(*[t.data_ptr() for t in ins])
+    out_arr = (ctypes.c_void_p * nsig)(*[t.data_ptr() for t in outs])
+    torch.cuda.synchronize()
+    _lib.call("fcwt_plan_execute_batched", h, in_arr, out_arr, fcwt.FCWT_OUT_C64)
+    _lib.call("fcwt_synchronize", ctx.handle)
+    assert rel_l2(outs[1].cpu().numpy(), oracle.cwt_fp64(xs[1], scs[1], 6.0, 1, True)) < 1e-5
+    ctx.close()
+    rc = lib.fcwt_plan_execute_batched(h, in_arr, out_arr, fcwt.FCWT_OUT_C64)
+    assert rc == _lib.FCWT_ERR_INVALID and b"context" in lib.fcwt_last_error()
+    assert lib.fcwt_plan_destroy(h) == 0
