@@ -29,7 +29,7 @@ cudaError_t launch_twiddle(int log2N, float2* tw, cudaStream_t st);
 cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
                            float2* out, float2* tmp, cudaStream_t st, int* n_kernels);
 cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
-                                   int* n_kernels);
+                                   int* n_kernels, bool real);
 cudaError_t launch_inverse_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
                                    int* n_kernels);
 cudaError_t launch_adjoint_accum(const float2* Xs, const float2* Gh, float2* H, const void* rows, int nr, int half,
@@ -767,7 +767,8 @@ int enqueue_forward(fcwt_plan* P, const void* const* din, const fcwt::FwdJob* gr
         for (auto& g : groups) {
             int n_fwd = 0;
             FCWT_CUDA_TRY(launch_forward_batched(djobs + off, g.second, P->tables[(size_t)g.first].log2N,
-                                                 P->tables[(size_t)g.first].tw.as<float2>(), st, &n_fwd));
+                                                 P->tables[(size_t)g.first].tw.as<float2>(), st, &n_fwd,
+                                                 !P->is_complex));
             ctx->kernel_launches += n_fwd;
             off += g.second;
         }
@@ -1721,7 +1722,7 @@ int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch
         j.tmp = ctx->adj_tmp.as<float2>() + (size_t)b * N;
     }
     FCWT_CUDA_TRY(cudaMemcpyAsync(jd + jo, jh + jo, (size_t)batch * sizeof(FwdJob), cudaMemcpyHostToDevice, st));
-    FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch, log2N, tw, st, &nk));
+    FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch, log2N, tw, st, &nk, true));
     ctx->kernel_launches += nk;
     jo += batch;
     // rows in chunks: Ghat = FFT(G), accumulate H and the parameter sums
@@ -1749,7 +1750,7 @@ int fcwt_morlet_cwt_backward(fcwt_context* ctx, const float* x, int n, int batch
             }
         }
         FCWT_CUDA_TRY(cudaMemcpyAsync(jd + jo, jh + jo, (size_t)batch * nr * sizeof(FwdJob), cudaMemcpyHostToDevice, st));
-        FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch * nr, log2N, tw, st, &nk));
+        FCWT_CUDA_TRY(launch_forward_batched(jd + jo, batch * nr, log2N, tw, st, &nk, false));
         ctx->kernel_launches += nk;
         jo += (size_t)batch * nr;
         FCWT_CUDA_TRY(launch_adjoint_accum(ctx->adj_x.as<float2>(), ctx->adj_g.as<float2>(), ctx->adj_h.as<float2>(),
