@@ -26,7 +26,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["fcwt_kernels.cu", "fcwt_tc.cu", "fcwt_capi.cu", "fcwt_noalloc.cu", "fcwt_adjoint.cu"]
+CU_SOURCES = ["fcwt_kernels.cu", "fcwt_fwd.cu", "fcwt_tc.cu", "fcwt_capi.cu", "fcwt_noalloc.cu", "fcwt_adjoint.cu"]
 CPP_SOURCES = ["fcwt_host.cpp", "fcwt_plan.cpp", "fcwt_cpp.cpp"]
 HEADERS = ["fcwt_internal.h", "fcwt_plan.h", "fcwt_fft.cuh", "fcwt_dev.cuh"]
 

@@ -4,12 +4,7 @@
 //                 src/fcwt/fcwt.cpp:51-67): float operations in the
 //                 reference's order, exp evaluated in float64 then rounded.
 //   k_twiddle     two-level twiddle table w_N^j (float64 sincospi, rounded).
-//   k_fwd_pass    one radix-R Stockham pass of the forward FFT of the
-//                 zero-padded input (replaces fftwf r2c / c2c FORWARD,
-//                 fcwt.cpp:486-500). A real signal runs as an N/2-point
-//                 complex FFT of its sample pairs, and k_r2c_post splits
-//                 that into all N bins, conjugate mirror included
-//                 (fcwt.cpp:507-510).
+//   (the forward FFT of the signal is in fcwt_fwd.cu)
 //   k_row_engine  persistent row engine: daughter multiply (fcwt.cpp:197-311),
 //                 inverse FFT (fcwt.cpp:418-429), normalisation
 //                 (fcwt.cpp:431-445) and crop to n (fcwt.cpp:396-416), fused,
@@ -54,134 +49,6 @@ __global__ void k_twiddle(int log2N, float2* __restrict__ tw) {
     double s, c;
     sincospi(2.0 * (double)e / (double)N, &s, &c);
     tw[j] = make_float2((float)c, (float)s);
-}
-
-// ------------------------------------------------------------- forward FFT
-
-// Element idx of the first pass's input with implicit zero padding: a
-// complex sample, or (r2c) the real pair (x[2 idx], x[2 idx + 1]).
-__device__ __forceinline__ float2 fwd_input(const float* __restrict__ in_r, const float2* __restrict__ in_c,
-                                            int n_in, int idx, int r2c) {
-    if (in_r && r2c) {
-        const int i0 = 2 * idx;
-        return make_float2(i0 < n_in ? __ldg(in_r + i0) : 0.0f, i0 + 1 < n_in ? __ldg(in_r + i0 + 1) : 0.0f);
-    }
-    if (idx >= n_in) return make_float2(0.0f, 0.0f);
-    return in_r ? make_float2(__ldg(in_r + idx), 0.0f) : __ldg(in_c + idx);
-}
-
-// One Stockham pass (natural order in and out after the last pass):
-//   k = j mod Ns; v_r = in[j + r N/R] * w^{-r k / (Ns R)}; V = DFT_R^-(v);
-//   out[(j - k) R + k + m Ns] = V_m.
-// The first pass reads the caller's signal with implicit zero padding. N is
-// the complex length; the twiddle table is that of 2^r2c N (r2c: the
-// N/2-point transform of a real signal's pairs uses every second entry).
-template <int R>
-__global__ void k_fwd_pass(const float2* __restrict__ in_c, const float* __restrict__ in_r, int n_in,
-                           int first, float2* __restrict__ out, int log2N, int log2Ns,
-                           const float2* __restrict__ tw, int r2c) {
-    const int N = 1 << log2N;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N / R) return;
-    const int Ns = 1 << log2Ns;
-    const int k = j & (Ns - 1);
-    const int shift = log2N - log2Ns - ilog2c(R) + r2c;  // table steps per w^{-1 / (Ns R)}
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        int idx = j + r * (N / R);
-        float2 a = first ? fwd_input(in_r, in_c, n_in, idx, r2c) : in_c[idx];
-        if (r > 0 && k > 0) {
-            float2 w = tw_lookup(tw, log2N + r2c, (unsigned)(r * k) << shift);
-            w.y = -w.y;
-            a = cmul(a, w);
-        }
-        v[r] = a;
-    }
-    fft_reg<R, -1>(v);
-    const int base = (j - k) * R + k;
-#pragma unroll
-    for (int m = 0; m < R; m++) out[base + m * Ns] = v[m];
-}
-
-
-// Batched Stockham pass: blockIdx.y selects the signal. src/dst: 0 = the
-// signal's input (first pass only), 1 = its spectrum X, 2 = its tmp buffer.
-// N and r2c as in k_fwd_pass.
-template <int R, int SIGN>
-__global__ void k_fwd_pass_batched(const FwdJob* __restrict__ jobs, int src_sel, int dst_sel, int log2N, int log2Ns,
-                                   const float2* __restrict__ tw, int r2c) {
-    const FwdJob J = jobs[blockIdx.y];
-    const int N = 1 << log2N;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N / R) return;
-    const int Ns = 1 << log2Ns;
-    const int k = j & (Ns - 1);
-    const int shift = log2N - log2Ns - ilog2c(R) + r2c;
-    const float2* src = src_sel == 1 ? J.X : J.tmp;
-    float2* dst = dst_sel == 1 ? J.X : J.tmp;
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const int idx = j + r * (N / R);
-        float2 a = src_sel == 0 ? fwd_input(J.in_r, J.in_c, J.n, idx, r2c) : src[idx];
-        if (r > 0 && k > 0) {
-            float2 w = tw_lookup(tw, log2N + r2c, (unsigned)(r * k) << shift);
-            if (SIGN < 0) w.y = -w.y;
-            a = cmul(a, w);
-        }
-        v[r] = a;
-    }
-    fft_reg<R, SIGN>(v);
-    const int base = (j - k) * R + k;
-#pragma unroll
-    for (int m = 0; m < R; m++) dst[base + m * Ns] = v[m];
-}
-
-// Real-input split: Z = FFT_{N/2} of z[j] = x[2j] + i x[2j+1] gives, with
-// E = (Z[k] + conj Z[N/2-k]) / 2 and O = -i (Z[k] - conj Z[N/2-k]) / 2,
-//   X[k] = E + w_N^{-k} O,   X[N/2 - k] = conj(E - w_N^{-k} O),
-// and X[N - k] = conj X[k] (real input). Thread k in [0, N/4] writes the
-// bins k, N/2 - k, N/2 + k and N - k, so all N bins are written once.
-__device__ __forceinline__ void r2c_split(const float2* __restrict__ Z, float2* __restrict__ X, int k, int log2N,
-                                          const float2* __restrict__ tw) {
-    const int N = 1 << log2N;
-    const int H = N >> 1;
-    const float2 A = Z[k];
-    const float2 Bz = Z[(H - k) & (H - 1)];
-    const float2 E = make_float2(0.5f * (A.x + Bz.x), 0.5f * (A.y - Bz.y));
-    const float2 O = make_float2(0.5f * (A.y + Bz.y), -0.5f * (A.x - Bz.x));
-    float2 w = tw_lookup(tw, log2N, (unsigned)k);
-    w.y = -w.y;
-    const float2 wo = cmul(w, O);
-    const float2 xk = make_float2(E.x + wo.x, E.y + wo.y);
-    const float2 yk = make_float2(E.x - wo.x, wo.y - E.y);
-    X[k] = xk;
-    if (k == 0) {
-        X[H] = yk;
-        return;
-    }
-    X[N - k] = make_float2(xk.x, -xk.y);
-    if (2 * k < H) {
-        X[H - k] = yk;
-        X[H + k] = make_float2(yk.x, -yk.y);
-    }
-}
-
-// Z (N/2 values) -> X (N bins) of one real signal.
-__global__ void k_r2c_post(const float2* __restrict__ Z, float2* __restrict__ X, int log2N,
-                           const float2* __restrict__ tw) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k > (1 << log2N) / 4) return;
-    r2c_split(Z, X, k, log2N, tw);
-}
-
-// Batched split: blockIdx.y selects the signal, Z in its tmp buffer.
-__global__ void k_r2c_post_batched(const FwdJob* __restrict__ jobs, int log2N, const float2* __restrict__ tw) {
-    const FwdJob J = jobs[blockIdx.y];
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k > (1 << log2N) / 4) return;
-    r2c_split(J.tmp, J.X, k, log2N, tw);
 }
 
 // --------------------------------------------------------------- row engine
@@ -828,136 +695,11 @@ cudaError_t launch_doublesided_combine(float2* out, const float2* V, long long r
     return cudaGetLastError();
 }
 
-// Radix sequence of a 2^log2C-point FFT: 16s, then one smaller pass.
-static int radix_plan(int log2C, int* radices) {
-    int np = 0, rem = log2C;
-    while (rem >= 4) {
-        radices[np++] = 16;
-        rem -= 4;
-    }
-    if (rem == 3) radices[np++] = 8;
-    if (rem == 2) radices[np++] = 4;
-    if (rem == 1) radices[np++] = 2;
-    return np;
-}
-
-cudaError_t launch_forward(const float* in_r, const float2* in_c, int n, int log2N, const float2* tw,
-                           float2* out, float2* tmp, cudaStream_t st, int* n_kernels) {
-    const int N = 1 << log2N;
-    *n_kernels = 0;
-    if (log2N == 0) {
-        // N == 1: the DFT is the identity (one sample or none).
-        cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float2), st);
-        if (e != cudaSuccess) return e;
-        if (n >= 1) {
-            if (in_r)
-                e = cudaMemcpy2DAsync(out, sizeof(float2), in_r, sizeof(float), sizeof(float), 1,
-                                      cudaMemcpyDeviceToDevice, st);
-            else
-                e = cudaMemcpyAsync(out, in_c, sizeof(float2), cudaMemcpyDeviceToDevice, st);
-        }
-        return e;
-    }
-    // a real signal (N >= 4): N/2-point FFT of its sample pairs, then the split
-    const int r2c = (in_r && log2N >= 2) ? 1 : 0;
-    const int log2C = log2N - r2c;  // complex transform length
-    const int C = 1 << log2C;
-    int radices[32];
-    const int np = radix_plan(log2C, radices);
-    // ping-pong so that the last pass lands in `out` (r2c: in `tmp`, split into `out`)
-    float2* bufs[2] = {out, tmp};
-    int cur = ((np + r2c) % 2 == 1) ? 0 : 1;
-    const float2* src_c = in_c;
-    const float* src_r = in_r;
-    int log2Ns = 0;
-    for (int p = 0; p < np; p++) {
-        const int R = radices[p];
-        float2* dst = bufs[cur];
-        const int threads = C / R;
-        const int tb = threads < 256 ? threads : 256;
-        const int grid = (threads + tb - 1) / tb;
-        const int first = p == 0 ? 1 : 0;
-        switch (R) {
-            case 16: dev::k_fwd_pass<16><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2C, log2Ns, tw, r2c); break;
-            case 8: dev::k_fwd_pass<8><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2C, log2Ns, tw, r2c); break;
-            case 4: dev::k_fwd_pass<4><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2C, log2Ns, tw, r2c); break;
-            default: dev::k_fwd_pass<2><<<grid, tb, 0, st>>>(src_c, src_r, n, first, dst, log2C, log2Ns, tw, r2c); break;
-        }
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        (*n_kernels)++;
-        src_c = dst;
-        src_r = nullptr;
-        log2Ns += dev::ilog2c(R);
-        cur ^= 1;
-    }
-    if (r2c) {
-        const int threads = N / 4 + 1;
-        dev::k_r2c_post<<<(threads + 255) / 256, 256, 0, st>>>(tmp, out, log2N, tw);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        (*n_kernels)++;
-    }
-    return cudaSuccess;
-}
-
-// Forward FFTs of njobs signals of the same padded length 2^log2N. real:
-// every job's input is real (in_r), run as r2c (N >= 4).
-template <int SIGN>
-cudaError_t launch_fft_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
-                               int* n_kernels, bool real) {
-    *n_kernels = 0;
-    if (njobs <= 0) return cudaSuccess;
-    if (log2N == 0) return cudaErrorInvalidValue;  // N == 1 is handled by the single-signal path
-    const int r2c = (SIGN < 0 && real && log2N >= 2) ? 1 : 0;
-    const int log2C = log2N - r2c;
-    const int C = 1 << log2C;
-    int radices[32];
-    const int np = radix_plan(log2C, radices);
-    int log2Ns = 0;
-    int src = 0;
-    for (int p = 0; p < np; p++) {
-        const int R = radices[p];
-        // the last pass lands in X (r2c: in tmp, split into X)
-        const int dst = ((np - 1 - p + r2c) % 2 == 0) ? 1 : 2;
-        const int threads = C / R;
-        const int tb = threads < 256 ? threads : 256;
-        dim3 grid((threads + tb - 1) / tb, njobs);
-        switch (R) {
-            case 16: dev::k_fwd_pass_batched<16, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2C, log2Ns, tw, r2c); break;
-            case 8: dev::k_fwd_pass_batched<8, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2C, log2Ns, tw, r2c); break;
-            case 4: dev::k_fwd_pass_batched<4, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2C, log2Ns, tw, r2c); break;
-            default: dev::k_fwd_pass_batched<2, SIGN><<<grid, tb, 0, st>>>(jobs, src, dst, log2C, log2Ns, tw, r2c); break;
-        }
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        (*n_kernels)++;
-        src = dst;
-        log2Ns += dev::ilog2c(R);
-    }
-    if (r2c) {
-        const int threads = (1 << log2N) / 4 + 1;
-        dev::k_r2c_post_batched<<<dim3((threads + 255) / 256, njobs), 256, 0, st>>>(jobs, log2N, tw);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        (*n_kernels)++;
-    }
-    return cudaSuccess;
-}
-
-cudaError_t launch_forward_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
-                                   int* n_kernels, bool real) {
-    return launch_fft_batched<-1>(jobs, njobs, log2N, tw, st, n_kernels, real);
-}
-
-// Inverse (sign +, unnormalised) batched FFTs of complex inputs, same job layout.
-cudaError_t launch_inverse_batched(const FwdJob* jobs, int njobs, int log2N, const float2* tw, cudaStream_t st,
-                                   int* n_kernels) {
-    return launch_fft_batched<+1>(jobs, njobs, log2N, tw, st, n_kernels, false);
-}
+cudaError_t fft_configure();
 
 cudaError_t engine_configure() {
-    cudaError_t e;
+    cudaError_t e = fft_configure();
+    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(dev::k_row_engine<OUT_C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)dev::kEngineSmemBytes);
     if (e != cudaSuccess) return e;

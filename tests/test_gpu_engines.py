@@ -212,7 +212,12 @@ def test_tuner_records_engine_choice(fcwt, oracle, ctx, tmp_path, monkeypatch):
 @pytest.mark.parametrize("n", [100000, 30001], ids=["tensor_map_stores", "plain_stores"])
 def test_power_and_db_epilogues(fcwt, oracle, ctx, mode, n):
     """FCWT_OUT_POWER (|W|^2) and FCWT_OUT_DB (10 log10 |W|^2) written by the
-    row kernels equal the squared magnitude of the float64 oracle."""
+    row kernels: both equal |W|^2 of the same plan's complex64 output W up to
+    the epilogue's own float32 rounding, and the squared magnitude of the
+    float64 oracle within the float32 transform's error. That error is absolute
+    (about 1e-7 of the row's peak amplitude), so the dB comparison with the
+    oracle covers the elements within 40 dB of the peak, where it is below
+    1e-3 dB; the comparison with W covers every element above 1e-30."""
     from fcwt_b200 import _lib
 
     m = _lib.FCWT_ENGINE_TENSOR_CORES if mode == "tensor_cores" else _lib.FCWT_ENGINE_CUDA_CORES
@@ -222,13 +227,19 @@ def test_power_and_db_epilogues(fcwt, oracle, ctx, mode, n):
     ref = np.abs(oracle.cwt_fp64(x, sc, 2.0, 1, True)) ** 2
     ctx.set_engine(m)
     p = fcwt.Plan(n, sc, fb=2.0, threads=1, norm=True)
+    w = np.zeros((24, n), np.complex64)
     pw = np.zeros((24, n), np.float32)
     db = np.zeros((24, n), np.float32)
+    p.execute(x, w)
     p.execute(x, pw, out_type=fcwt.FCWT_OUT_POWER)
     p.execute(x, db, out_type=fcwt.FCWT_OUT_DB)
     p.close()
+    w2 = np.abs(w.astype(np.complex128)) ** 2
+    assert np.max(np.abs(pw - w2) / np.maximum(w2, 1e-30)) < 1e-5
+    own = w2 > 1e-30
+    assert np.max(np.abs(db[own] - 10 * np.log10(w2[own]))) < 1e-4
     assert np.linalg.norm(pw - ref) / np.linalg.norm(ref) < 2e-5
-    mask = ref > 1e-6 * ref.max()
+    mask = ref > 1e-4 * ref.max()
     assert np.max(np.abs(db[mask] - 10 * np.log10(ref[mask]))) < 1e-3
 
 
