@@ -246,7 +246,12 @@ def main():
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "grad", "long"],
                     help="plain: the 100k x 3000 transform with all forms (default); batched / grad / long: "
                          "only that form, as its own JSON line")
+    ap.add_argument("--skip-loop", action="store_true",
+                    help="--workload batched: time only the batched plan, not the per-channel loop beside it "
+                         "(profiling captures)")
     args = ap.parse_args()
+    if args.skip_loop and args.workload != "batched":
+        ap.error("--skip-loop applies to --workload batched")
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -518,7 +523,7 @@ def _batched_check_channels(ns) -> list[int]:
     return sorted(set(picks))
 
 
-def form_batched(steps: int, warmup: int, stream, check: bool = True) -> dict:
+def form_batched(steps: int, warmup: int, stream, check: bool = True, loop_baseline: bool = True) -> dict:
     import torch
 
     import fcwt_b200 as fcwt
@@ -540,7 +545,7 @@ def form_batched(steps: int, warmup: int, stream, check: bool = True) -> dict:
     def batched():
         bp.execute(xs, outs, graph=True, stream=stream)
 
-    ms_loop = _timed(loop, steps, warmup, stream)
+    ms_loop = _timed(loop, steps, warmup, stream) if loop_baseline else None
     for p in plans:
         p.close()
     ms_b = _timed(batched, steps, warmup, stream)
@@ -553,8 +558,8 @@ def form_batched(steps: int, warmup: int, stream, check: bool = True) -> dict:
                       "channels": C, "points": points, "output_bytes": 8 * points,
                       "rows": st["rows"], "tensor_core_rows": st["tensor_core_rows"]},
            "plain_loop": {"value": points / (ms_loop / 1e3), "ms_per_step": ms_loop,
-                          "what": "one plan per channel executed in a loop on one stream"},
-           "speedup_vs_plain_loop": ms_loop / ms_b,
+                          "what": "one plan per channel executed in a loop on one stream"} if ms_loop else None,
+           "speedup_vs_plain_loop": ms_loop / ms_b if ms_loop else None,
            "hbm_gbs": 8 * points / (ms_b / 1e3) / 1e9}
     if check:
         from oracle.oracle import Restatement
@@ -712,7 +717,7 @@ def run_form(args) -> None:
     sampler = ClockSampler(dev)
     fn = {"batched": form_batched, "grad": form_grad, "long": form_long}[args.workload]
     sampler.start()
-    res = fn(steps, warmup, stream)
+    res = fn(steps, warmup, stream, loop_baseline=False) if args.skip_loop else fn(steps, warmup, stream)
     clocks = sampler.stop()
     line = {"n_gpus": 1, "steps": steps, "warmup": warmup, "data": "synthetic", "scaling": "weak",
             "vs_baseline": None, "higher_is_better": True, "dtype": "f32"}

@@ -812,8 +812,8 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
         else
             map_ok = encode_output_map16(dout[0], S.n_out(), S.sp.M / S.dec, S.rows_out(), &omap) ? 1 : 0;
     }
-    // the CUDA-core engine stages complex64 boxes only
-    ep.tma_store = (P->two_phase && out_type == FCWT_OUT_C64) ? map_ok : 0;
+    // the CUDA-core engine's two-phase rows store through the same map
+    ep.tma_store = P->two_phase ? map_ok : 0;
     const int grid = std::max(1, std::min(P->n_items, ctx->engine_ctas));
     if (P->n_tc > 0) {
         TcParams tp;

@@ -32,7 +32,7 @@
 namespace fcwt {
 namespace dev {
 
-constexpr int kFftThreads = 256;
+constexpr int kFftThreads = 128;
 constexpr int kFftMaxLog2Tile = 12;  // B L <= 4096 complex values per CTA (2 x 32 KB)
 constexpr int kFftSmemBytes = 2 * (1 << kFftMaxLog2Tile) * 8;
 constexpr int kFftTargetCtas = 2 * 148;  // about two CTAs per SM of a B200
@@ -57,17 +57,24 @@ __device__ __forceinline__ float2 fft_tw(const float2* __restrict__ tw, int log2
     return w;
 }
 
+// w_L^{SIGN e}, e < L, from the CTA's two-level table of w_L^{SIGN j}:
+// tl[j] for j < 64 and th[j] = w_L^{SIGN 64 j} for j < L / 64.
+__device__ __forceinline__ float2 stage_tw(const float2* __restrict__ tl, const float2* __restrict__ th, unsigned e) {
+    return e < 64u ? tl[e] : cmul(tl[e & 63u], th[e >> 6]);
+}
+
 // One radix-R Stockham stage over L = 2^log2L points of B = 2^log2B
 // interleaved columns: k = j mod Ns, v_r = in[j + r L/R] w_{Ns R}^{SIGN r k},
 // V = DFT_R(v), out[(j - k) R + k + m Ns] = V_m.
 template <int R, int SIGN>
 __device__ __forceinline__ void smem_stage(const float2* __restrict__ in, float2* __restrict__ out, int log2L,
-                                           int log2B, int log2Ns, const float2* __restrict__ tw, int log2T) {
+                                           int log2B, int log2Ns, const float2* __restrict__ tl,
+                                           const float2* __restrict__ th) {
     constexpr int LR = ilog2c(R);
     const int B = 1 << log2B;
     const int Lr = 1 << (log2L - LR);
     const int tasks = Lr << log2B;
-    const int shift = log2T - log2Ns - LR;
+    const int shift = log2L - log2Ns - LR;  // w_{Ns R} = w_L^{2^shift}
     for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
         const int cc = t & (B - 1);
         const int j = t >> log2B;
@@ -76,7 +83,7 @@ __device__ __forceinline__ void smem_stage(const float2* __restrict__ in, float2
 #pragma unroll
         for (int r = 0; r < R; r++) {
             float2 x = in[((j + r * Lr) << log2B) + cc];
-            if (r > 0 && k > 0) x = cmul(x, fft_tw<SIGN>(tw, log2T, (unsigned)(r * k) << shift));
+            if (r > 0 && k > 0) x = cmul(x, stage_tw(tl, th, (unsigned)(r * k) << shift));
             v[r] = x;
         }
         fft_reg<R, SIGN>(v);
@@ -89,16 +96,16 @@ __device__ __forceinline__ void smem_stage(const float2* __restrict__ in, float2
 // All stages of an L-point FFT on the tile in `a` (natural order in and
 // out); returns the buffer that holds the result.
 template <int SIGN>
-__device__ __forceinline__ float2* smem_fft(float2* a, float2* b, int log2L, int log2B, const float2* __restrict__ tw,
-                                            int log2T) {
+__device__ __forceinline__ float2* smem_fft(float2* a, float2* b, int log2L, int log2B, const float2* __restrict__ tl,
+                                            const float2* __restrict__ th) {
     int log2Ns = 0;
     while (log2Ns < log2L) {
         const int lr = min(4, log2L - log2Ns);
         switch (lr) {
-            case 4: smem_stage<16, SIGN>(a, b, log2L, log2B, log2Ns, tw, log2T); break;
-            case 3: smem_stage<8, SIGN>(a, b, log2L, log2B, log2Ns, tw, log2T); break;
-            case 2: smem_stage<4, SIGN>(a, b, log2L, log2B, log2Ns, tw, log2T); break;
-            default: smem_stage<2, SIGN>(a, b, log2L, log2B, log2Ns, tw, log2T); break;
+            case 4: smem_stage<16, SIGN>(a, b, log2L, log2B, log2Ns, tl, th); break;
+            case 3: smem_stage<8, SIGN>(a, b, log2L, log2B, log2Ns, tl, th); break;
+            case 2: smem_stage<4, SIGN>(a, b, log2L, log2B, log2Ns, tl, th); break;
+            default: smem_stage<2, SIGN>(a, b, log2L, log2B, log2Ns, tl, th); break;
         }
         __syncthreads();
         float2* s = a;
@@ -123,6 +130,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cols(const FwdJob* __restri
                                                           int dst_sel, int log2C, int log2L, int log2B, int mode,
                                                           int r2c, const float2* __restrict__ tw, int log2T) {
     extern __shared__ float2 fft_sm[];
+    __shared__ float2 tl[64], th[64];
     const FwdJob J = jobs ? jobs[blockIdx.y] : one;
     const int L = 1 << log2L;
     const int B = 1 << log2B;
@@ -132,6 +140,11 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cols(const FwdJob* __restri
     float2* a = fft_sm;
     float2* b = fft_sm + tot;
     const float2* src = src_sel == 1 ? J.X : J.tmp;
+    // stage twiddles w_L^{SIGN j}: tl for j < 64, th for multiples of 64
+    for (int t = threadIdx.x; t < 128; t += kFftThreads) {
+        const unsigned e = t < 64 ? (unsigned)t : (unsigned)(t - 64) << 6;
+        if (e < (unsigned)L) (t < 64 ? tl[t] : th[t - 64]) = fft_tw<SIGN>(tw, log2T, e << (log2T - log2L));
+    }
     for (int t = threadIdx.x; t < tot; t += kFftThreads) {
         int i, cc;
         if (mode == 0) {
@@ -146,7 +159,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_cols(const FwdJob* __restri
         a[(i << log2B) + cc] = src_sel == 0 ? fwd_input(J.in_r, J.in_c, J.n, j, r2c) : src[j];
     }
     __syncthreads();
-    const float2* res = smem_fft<SIGN>(a, b, log2L, log2B, tw, log2T);
+    const float2* res = smem_fft<SIGN>(a, b, log2L, log2B, tl, th);
     float2* dst = dst_sel == 1 ? J.X : J.tmp;
     for (int t = threadIdx.x; t < tot; t += kFftThreads) {
         const int cc = t & (B - 1);

@@ -375,23 +375,35 @@ __device__ __forceinline__ void phase2_item(const float2* __restrict__ G, int c0
     const long long row0 = out_off + c0;
     if (tma) {
         unsigned char* stage = reinterpret_cast<unsigned char*>(region0);
+        if constexpr (OT == OUT_C64) {
 #pragma unroll
-        for (int h = 0; h < 32; h++)
-            *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * h, warp)) = x[h];
+            for (int h = 0; h < 32; h++)
+                *reinterpret_cast<float2*>(stage + stage_off(lane + 32 * h, warp)) = x[h];
+        } else {
+#pragma unroll
+            for (int h = 0; h < 32; h++)
+                *reinterpret_cast<unsigned*>(stage + stage16_off(lane + 32 * h, warp)) = pack16<OT>(x[h]);
+        }
         fence_proxy_async_smem();
         __syncthreads();
         const int n_full = n / M;  // stripes a < n_full are complete
+        constexpr int box_bytes = OT == OUT_C64 ? kBoxBytes : kBoxBytes / 2;
         if (tid == 0) {
-            // output lines evict-first in L2: they are not read again, and the
-            // spectrum and scratch the engine re-reads stay resident
+            // complex64 output lines evict-first in L2: they are not read again,
+            // and the spectrum and scratch the engine re-reads stay resident
             for (int j = 0; j < 4 && j * kBoxRows < n_full; j++)
-                tma_store_3d<true>(omap, stage + j * kBoxBytes, c0, j * kBoxRows, out_row);
+                tma_store_3d<OT == OUT_C64>(omap, stage + j * box_bytes, c0, j * kBoxRows, out_row);
             bulk_commit();
         }
         const int tail = n - n_full * M;  // samples of the partial stripe a = n_full
-        if (tid < kGroupCols && c0 + tid < tail && n_full < kP2)
-            store_out<OT>(outb, row0 + tid + (long long)M * n_full,
-                          *reinterpret_cast<const float2*>(stage + stage_off(n_full, tid)));
+        if (tid < kGroupCols && c0 + tid < tail && n_full < kP2) {
+            const long long o = row0 + tid + (long long)M * n_full;
+            if constexpr (OT == OUT_C64)
+                store_out<OT>(outb, o, *reinterpret_cast<const float2*>(stage + stage_off(n_full, tid)));
+            else
+                __stcs(reinterpret_cast<unsigned*>(outb) + o,
+                       *reinterpret_cast<const unsigned*>(stage + stage16_off(n_full, tid)));
+        }
         // region0 is reused only after thread 0 waited for the bulk reads
     } else {
 #pragma unroll
@@ -561,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (s_ok) {
                 const float2* G = P.scratch + (size_t)R.slot * (size_t)P.slot_elems;
                 phase2_item<OT>(G, item.part * kGroupCols, (N >> kLog2P2) / R.dec, R.n_out, R.dec, outb, R.out_off,
-                                R.out_row, region0, t2, &omap, P.tma_store != 0 && OT == OUT_C64 && R.out_buf == 0);
+                                R.out_row, region0, t2, &omap, P.tma_store != 0 && R.out_buf == 0);
                 if (tid == 0) {
                     __threadfence();
                     red_release_add(b_done + item.row, 1u);
