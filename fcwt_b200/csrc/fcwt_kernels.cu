@@ -242,7 +242,10 @@ __device__ void phase1_wide(const SigDesc& S, const RowDesc& R, const float* __r
 // K2-point DFT over j per (v, u1, k2) task; every thread works in both steps.
 // The spectrum x weights of the 8 k2 columns are loaded into SMEM once per
 // item (zt[k1][8]); the FFT32 outputs of a batch of v values go through SMEM
-// (Y[u1][task], padded rows). Outputs: G[c = v + R u][k2] w_N^{(k2+L) c}.
+// (Y[u1][task], padded rows). When the step-B tasks of all v are exactly one
+// per thread (M = 1024, any K), all v run as one batch and Y overwrites zt
+// once every thread holds its inputs in registers. Outputs:
+// G[c = v + R u][k2] w_N^{(k2+L) c}.
 template <int K2>
 __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
                            const float2* __restrict__ twlo, const float2* __restrict__ twhi,
@@ -262,37 +265,53 @@ __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __re
     const int Rr = M / K;
     const float nm1 = (float)N - 1.0f;
     float2* zt = region0;
-    float2* Y = region0 + K * W;
+    const bool whole = Rr * K2 * W == kThreads;
+    static_assert(32 * (kThreads + kYPad) <= kRegion0, "one batch of Y over zt fits in region0");
+    float2* Y = whole ? region0 : region0 + K * W;
+    const int VBn = whole ? Rr : VBmax;
     for (int idx = tid; idx < K * W; idx += kThreads) {
         const int k1 = idx >> 3;
         const int kk = idx & 7;
         zt[idx] = bin_value(R, S, pool, nm1, R.L + k2_0 + kk + kP2 * k1);
     }
     __syncthreads();
-    for (int v0 = 0; v0 < Rr; v0 += VBmax) {
-        const int VB = min(VBmax, Rr - v0);
+    // (B) task t = (vb K2 + j) 8 + kk: FFT32 over i of the pre-twiddled column,
+    // then the twiddle w_K^{j u1} = w_M^{j u1 R}
+    auto fft32_task = [&](int t, int v0, float2 (&x)[32]) {
+        const int kk = t & 7;
+        const int j = (t >> 3) % K2;
+        const int v = v0 + (t >> 3) / K2;
+        // pre-twiddle w_M^{v k1}: exact table value every 8 steps, running product in between
+        const float2 stp = twhi[((unsigned)v * (unsigned)K2) & Mm];
+        float2 w = make_float2(1.0f, 0.0f);
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            if ((i & 7) == 0) w = twhi[((unsigned)v * (unsigned)(j + K2 * i)) & Mm];
+            x[i] = cmul(zt[(j + K2 * i) * W + kk], w);
+            w = cmul(w, stp);
+        }
+        fft_reg<32, +1>(x);
+#pragma unroll
+        for (int u1 = 1; u1 < 32; u1++) x[u1] = cmul(x[u1], twhi[((unsigned)(j * u1 * Rr)) & Mm]);
+    };
+    for (int v0 = 0; v0 < Rr; v0 += VBn) {
+        const int VB = min(VBn, Rr - v0);
         const int T = VB * K2 * W;
         const int TP = T + kYPad;
-        // (B) FFT32 over i, task t = (vb K2 + j) 8 + kk
-        for (int t = tid; t < T; t += kThreads) {
-            const int kk = t & 7;
-            const int j = (t >> 3) % K2;
-            const int v = v0 + (t >> 3) / K2;
-            // pre-twiddle w_M^{v k1}: exact table value every 8 steps, running product in between
-            const float2 stp = twhi[((unsigned)v * (unsigned)K2) & Mm];
-            float2 w = make_float2(1.0f, 0.0f);
+        if (whole) {
+            // one task per thread; Y overwrites zt after every thread has read its inputs
             float2 x[32];
+            fft32_task(tid, v0, x);
+            __syncthreads();
 #pragma unroll
-            for (int i = 0; i < 32; i++) {
-                if ((i & 7) == 0) w = twhi[((unsigned)v * (unsigned)(j + K2 * i)) & Mm];
-                x[i] = cmul(zt[(j + K2 * i) * W + kk], w);
-                w = cmul(w, stp);
+            for (int u1 = 0; u1 < 32; u1++) Y[u1 * TP + tid] = x[u1];
+        } else {
+            for (int t = tid; t < T; t += kThreads) {
+                float2 x[32];
+                fft32_task(t, v0, x);
+#pragma unroll
+                for (int u1 = 0; u1 < 32; u1++) Y[u1 * TP + t] = x[u1];
             }
-            fft_reg<32, +1>(x);
-            // twiddle w_K^{j u1} = w_M^{j u1 R}
-            Y[t] = x[0];
-#pragma unroll
-            for (int u1 = 1; u1 < 32; u1++) Y[u1 * TP + t] = cmul(x[u1], twhi[((unsigned)(j * u1 * Rr)) & Mm]);
         }
         __syncthreads();
         // (C) K2-point DFT over j, task t = (vb 32 + u1) 8 + kk
