@@ -59,11 +59,13 @@ __global__ void k_twiddle(int log2N, float2* __restrict__ tw) {
 //   zs:      phase-1 input tile [K][kChunk]
 //   twlo:    w_N^j, j < 1024, of the current N
 //   t2:      w_1024^{a l} at [a*32 + l]
-//   twhi:    w_N^{1024 j}, j < M, of the current N (when M <= 512)
+//   twhi:    w_N^{1024 j} = w_M^j, j < M, of the current N (M <= 512), or
+//            w_M^j for j < 32 followed by w_M^{32 j} for j < M / 32 (M > 512)
 constexpr int kStagePitch = kGroupCols + 1;
 constexpr int kRegion0 = kP2 * kStagePitch;
 constexpr int kZs = kChunk * kMaxK;
 constexpr int kTwhiSmem = 512;
+static_assert(32 + (1 << (kMaxLog2N - kLog2P2)) / 32 <= kTwhiSmem, "split w_M tables of the largest N fit");
 constexpr int kSmemFloat2 = kRegion0 + kZs + kP2 + kP2 + kTwhiSmem;
 constexpr size_t kSmemAlign = 1024;  // the 64B-swizzled staging tile wants 1 KB alignment
 constexpr size_t kEngineSmemBytes = (size_t)kSmemFloat2 * sizeof(float2) + kSmemAlign;
@@ -100,13 +102,28 @@ __device__ bool wait_counter(const unsigned* p, unsigned target, int* err) {
     return true;
 }
 
+// w_M^x (x < M) of the current N from shared memory: the table itself when
+// M <= kTwhiSmem, otherwise the product of a[x mod 32] = w_M^{x mod 32} and
+// b[x / 32] = w_M^{32 (x / 32)} (32 + M / 32 <= 288 entries for M <= 8192).
+struct TwM {
+    const float2* a;
+    const float2* b;  // null: a is the whole table
+    __device__ __forceinline__ float2 operator[](unsigned x) const {
+        return b ? cmul(a[x & 31u], b[x >> 5]) : a[x];
+    }
+};
+// w_N^e with e < N from the low table w_N^j (j < 1024) and w_M.
+__device__ __forceinline__ float2 tw_n(const float2* __restrict__ twlo, const TwM& twhi, unsigned e) {
+    return cmul(twlo[e & 1023u], twhi[e >> 10]);
+}
+
 // Phase 1 of one chunk of kChunk k2 values of a row (see fcwt_internal.h):
 // loads Z into the tile zs[k1][k2], then every (k2, v) task runs a K-point
 // DFT and writes G[c][k2] (c = v + R u) times w_N^{(k2+L) c}.
 template <int K, bool TO_GLOBAL>
 __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
                              float2* __restrict__ zs, const float2* __restrict__ twlo,
-                             const float2* __restrict__ twhi, float2* __restrict__ gdst) {
+                             const TwM twhi, float2* __restrict__ gdst) {
     const int tid = threadIdx.x;
     const int log2N = S.log2N;
     const int N = 1 << log2N;
@@ -164,7 +181,7 @@ __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R,
 
 template <bool TO_GLOBAL>
 __device__ void phase1_chunk_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool,
-                                      int k2_0, float2* zs, const float2* twlo, const float2* twhi,
+                                      int k2_0, float2* zs, const float2* twlo, const TwM twhi,
                                       float2* gdst) {
     switch (K) {
         case 1: phase1_chunk<1, TO_GLOBAL>(S, R, pool, k2_0, zs, twlo, twhi, gdst); break;
@@ -183,7 +200,7 @@ __device__ void phase1_chunk_dispatch(int K, const SigDesc& S, const RowDesc& R,
 // G[v + R u][k2_0 .. k2_0+7] in 64-byte runs with the w_N^{(k2+L) c} twiddle.
 template <int K2>
 __device__ void phase1_wide(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
-                            const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                            const float2* __restrict__ twlo, const TwM twhi,
                             float2* __restrict__ region0, float2* __restrict__ G) {
     constexpr int K = 32 * K2;
     const int tid = threadIdx.x;
@@ -248,7 +265,7 @@ __device__ void phase1_wide(const SigDesc& S, const RowDesc& R, const float* __r
 // G[c = v + R u][k2] w_N^{(k2+L) c}.
 template <int K2>
 __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __restrict__ pool, int k2_0,
-                           const float2* __restrict__ twlo, const float2* __restrict__ twhi,
+                           const float2* __restrict__ twlo, const TwM twhi,
                            float2* __restrict__ region0, float2* __restrict__ G) {
     constexpr int K = 32 * K2;
     constexpr int W = kWideChunk;
@@ -342,7 +359,7 @@ __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __re
 }
 
 __device__ void phase1_wide_dispatch(int K, const SigDesc& S, const RowDesc& R, const float* pool, int k2_0,
-                                     const float2* twlo, const float2* twhi, float2* region0, float2* G) {
+                                     const float2* twlo, const TwM twhi, float2* region0, float2* G) {
     switch (K) {
         case 64: phase1_big<2>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
         case 128: phase1_big<4>(S, R, pool, k2_0, twlo, twhi, region0, G); break;
@@ -498,7 +515,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int n = S.n;
         void* outb = P.outs[R.out_buf];
         const int Mcols = N >> kLog2P2;
-        const float2* twhi = (Mcols <= kTwhiSmem) ? twhi_s : S.tw + kP2;
+        const TwM twhi = Mcols <= kTwhiSmem ? TwM{twhi_s, nullptr} : TwM{twhi_s, twhi_s + 32};
 
         // region0 may still be read by the bulk stores of the previous phase-2 item
         if (P.tma_store && (item.type == ITEM_PHASE2 || item.type == ITEM_FUSED || item.type == ITEM_PHASE1W)) {
@@ -508,7 +525,12 @@ __global__ void __launch_bounds__(kThreads, 2)
         // twiddle tables of this N into SMEM
         if (s_log2N != log2N) {
             for (int j = tid; j < kP2; j += kThreads) twlo[j] = S.tw[j];
-            for (int j = tid; j < Mcols && Mcols <= kTwhiSmem; j += kThreads) twhi_s[j] = S.tw[kP2 + j];
+            if (Mcols <= kTwhiSmem) {
+                for (int j = tid; j < Mcols; j += kThreads) twhi_s[j] = S.tw[kP2 + j];
+            } else {
+                for (int j = tid; j < 32; j += kThreads) twhi_s[j] = S.tw[kP2 + j];
+                for (int j = tid; j < Mcols / 32; j += kThreads) twhi_s[32 + j] = S.tw[kP2 + 32 * j];
+            }
             __syncthreads();
             if (tid == 0) s_log2N = log2N;
         }
