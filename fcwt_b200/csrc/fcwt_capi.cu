@@ -16,6 +16,7 @@
 #include <array>
 #include <map>
 #include <initializer_list>
+#include <queue>
 #include <vector>
 
 #include "../../include/fcwt_b200.h"
@@ -261,6 +262,8 @@ struct fcwt_plan {
     std::vector<PlanSignal> sig;
     std::vector<PlanTables> tables;
     DevBuf pool, sigs, rows, items, fwd_jobs, fwd_tmp, graph_jobs, tc_rows, tc_wts;
+    DevBuf tc_units;  // work list of the tensor-core engine (rows, the last ones possibly split)
+    int n_units = 0;
     // Per-execution uploads of batched plans (forward jobs, per-output tensor
     // maps) go through a ring of pinned host slots; a slot is rewritten only
     // after the copy that read it has run (its event), so back-to-back
@@ -320,6 +323,7 @@ void plan_release(fcwt_plan* p) {
     p->fwd_tmp.release();
     p->graph_jobs.release();
     p->tc_rows.release();
+    p->tc_units.release();
     p->tc_wts.release();
     p->Xs.release();
     p->sigs2.release();
@@ -350,6 +354,67 @@ void plan_free(fcwt_plan* p) {
     }
     plan_release(p);
     delete p;
+}
+
+// Finish time of a queue of work units on `ctas` persistent CTAs that claim
+// them in order (the earliest free CTA takes the next unit).
+double queue_makespan(const std::vector<double>& cost, int ctas) {
+    std::priority_queue<double, std::vector<double>, std::greater<double>> q;
+    for (int i = 0; i < ctas; i++) q.push(0.0);
+    double end = 0.0;
+    for (double c : cost) {
+        const double t = q.top() + c;
+        q.pop();
+        q.push(t);
+        end = std::max(end, t);
+    }
+    return end;
+}
+
+// Work list of the tensor-core engine: the rows in order, with the last K
+// rows split into 2, 4 or 8 parts of their column groups when a simulation of
+// the queue says that finishes sooner. Cost model in column-group times: a
+// unit costs its groups plus about 1.2 for the per-row pre-pass and prologue.
+std::vector<int> plan_tc_units(const std::vector<int>& tc_rows, const std::vector<int>& groups, int ctas) {
+    constexpr double kUnitOverhead = 1.2;
+    const int n = (int)tc_rows.size();
+    std::vector<int> best;
+    for (int g : tc_rows) best.push_back(g);
+    if (n == 0 || ctas <= 1) return best;
+    std::vector<double> cost;
+    for (int i = 0; i < n; i++) cost.push_back(kUnitOverhead + groups[(size_t)i]);
+    double best_t = queue_makespan(cost, ctas);
+    for (int lp = 1; lp <= 3; lp++) {
+        const int parts = 1 << lp;
+        for (int K : {ctas / 8, ctas / 4, ctas / 2, ctas, 2 * ctas}) {
+            K = std::min(K, n);
+            if (K <= 0) continue;
+            std::vector<int> units;
+            cost.clear();
+            for (int i = 0; i < n; i++) {
+                const int ng = groups[(size_t)i];
+                if (i < n - K || ng < 2 * parts) {
+                    units.push_back(tc_rows[(size_t)i]);
+                    cost.push_back(kUnitOverhead + ng);
+                    continue;
+                }
+                for (int part = 0; part < parts; part++) {
+                    const int e = fcwt::tc_unit(tc_rows[(size_t)i], lp, part);
+                    int gb, ge;
+                    fcwt::tc_unit_groups(e, ng, &gb, &ge);
+                    if (ge <= gb) continue;
+                    units.push_back(e);
+                    cost.push_back(kUnitOverhead + (ge - gb));
+                }
+            }
+            const double t = queue_makespan(cost, ctas);
+            if (t < best_t * 0.995) {
+                best_t = t;
+                best = units;
+            }
+        }
+    }
+    return best;
 }
 
 // Builds descriptors and the work list of all signals. Rows of N < 1024 get a
@@ -560,6 +625,16 @@ int plan_build(fcwt_plan* P) {
     if (!tc_rows.empty()) {
         FCWT_CUDA_TRY(P->tc_rows.ensure(tc_rows.size() * sizeof(int)));
         FCWT_CUDA_TRY(cudaMemcpyAsync(P->tc_rows.p, tc_rows.data(), tc_rows.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, st));
+        std::vector<int> groups;
+        for (int g : tc_rows) {
+            const RowDesc& d = rows[(size_t)g];
+            groups.push_back((1 << (P->sig[(size_t)d.sig].sp.log2N - kLog2P2)) / d.dec / kGroupCols);
+        }
+        const std::vector<int> units = plan_tc_units(tc_rows, groups, ctx->num_sms);
+        P->n_units = (int)units.size();
+        FCWT_CUDA_TRY(P->tc_units.ensure(units.size() * sizeof(int)));
+        FCWT_CUDA_TRY(cudaMemcpyAsync(P->tc_units.p, units.data(), units.size() * sizeof(int),
                                       cudaMemcpyHostToDevice, st));
         FCWT_CUDA_TRY(P->tc_wts.ensure((size_t)tc_wts_elems * sizeof(float)));
         DevBuf owners;
@@ -820,8 +895,8 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
         std::memset(&tp, 0, sizeof(tp));
         tp.sigs = ep.sigs;
         tp.rows = ep.rows;
-        tp.row_list = P->tc_rows.as<int>();
-        tp.n_list = P->n_tc;
+        tp.row_list = P->tc_units.as<int>();
+        tp.n_list = P->n_units;
         tp.stale_pool = ep.stale_pool;
         tp.wts = P->tc_wts.as<float>();
         tp.counter = ctx->counters.as<unsigned>() + n_counters - 1;
@@ -847,7 +922,7 @@ int enqueue_rows(fcwt_plan* P, const fcwt::SigDesc* dsigs, void* const* dout, in
             }
             tp.tma_store = 1;
         }
-        FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_tc, ctx->num_sms)), st));
+        FCWT_CUDA_TRY(launch_tc(tp, omap, out_type, std::max(1, std::min(P->n_units, ctx->num_sms)), st));
         ctx->kernel_launches += 1;
     }
     if (P->n_items > 0) {

@@ -121,10 +121,34 @@ struct EngineParams {
 constexpr int kTcMaxKp = 16;
 constexpr int kTcMinN = 16384;
 
+// Entries of the tensor-core engine's work list: a row index, or one of 2, 4
+// or 8 parts of a row's column groups (the last entries of a launch, so that
+// its final wave is finer than whole rows): row | log2(parts) << 24 | part << 26.
+constexpr int kUnitRowBits = 24;
+constexpr int kUnitRowMask = (1 << kUnitRowBits) - 1;
+__host__ __device__ constexpr int tc_unit(int row, int log2parts, int part) {
+    return row | (log2parts << kUnitRowBits) | (part << (kUnitRowBits + 2));
+}
+// Column groups [gb, ge) of a unit of a row with ng groups; part ranges hold an
+// even number of groups so that the two halves of a CTA share them evenly.
+__host__ __device__ inline void tc_unit_groups(int entry, int ng, int* gb, int* ge) {
+    const int lp = (entry >> kUnitRowBits) & 3;
+    const int part = (entry >> (kUnitRowBits + 2)) & 7;
+    if (lp == 0) {
+        *gb = 0;
+        *ge = ng;
+        return;
+    }
+    const int parts = 1 << lp;
+    const int chunk = (((ng + parts - 1) / parts) + 1) & ~1;
+    *gb = part * chunk < ng ? part * chunk : ng;
+    *ge = *gb + chunk < ng ? *gb + chunk : ng;
+}
+
 struct TcParams {
     const SigDesc* sigs;
     const RowDesc* rows;
-    const int* row_list;       // rows of this launch, in queue order
+    const int* row_list;       // work units of this launch (tc_unit entries), in queue order
     int n_list;
     const float* stale_pool;
     const float* wts;          // per-row daughter weights x out_scale on [L, L + 1024 kp)

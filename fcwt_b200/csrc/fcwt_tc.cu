@@ -44,6 +44,7 @@ namespace dev {
 
 constexpr int kTcThreads = 512;
 constexpr int kTcCols = 8;          // columns per group (one per warp of a half)
+static_assert(kTcCols == kGroupCols, "the planner counts tensor-core groups in kGroupCols");
 constexpr int kTcTmemCols = 512;
 constexpr int kTcDcol = 256;        // first accumulator column
 constexpr int kTcTwhiSmem = 512;    // w_M table kept in SMEM when M <= this
@@ -293,11 +294,14 @@ __device__ __forceinline__ float tc_prepass(const TcParams& P, const RowDesc& R,
 
 // Claims the CTA's next row from the queue into the other row slot and pulls
 // its weights and spectrum window into L2.
-__device__ __forceinline__ void tc_claim_next(const TcParams& P, int* next_idx, RowDesc* next_R, SigDesc* next_S) {
+__device__ __forceinline__ void tc_claim_next(const TcParams& P, int* next_idx, RowDesc* next_R, SigDesc* next_S,
+                                              int* next_unit) {
     const int i = (int)atomicAdd(P.counter, 1u);
     *next_idx = i;
     if (i < P.n_list) {
-        *next_R = P.rows[P.row_list[i]];
+        const int e = P.row_list[i];
+        *next_unit = e;
+        *next_R = P.rows[e & kUnitRowMask];
         *next_S = P.sigs[next_R->sig];
         const unsigned wb = (unsigned)(kP2 * next_R->kp) * 4u;
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(P.wts + next_R->woff), "r"(wb) : "memory");
@@ -314,7 +318,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
                                        const SigDesc& S, unsigned char* sm, const float2* __restrict__ twlo,
                                        const float2* __restrict__ twhi, const float2* __restrict__ t2, uint32_t tmem,
                                        uint32_t mbar_h, uint32_t& phase, float* s_red, int* next_idx,
-                                       RowDesc* next_R, SigDesc* next_S, bool kp16) {
+                                       RowDesc* next_R, SigDesc* next_S, int* next_unit, int unit, bool kp16) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -335,6 +339,8 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
 
     // ---- column groups
     const int ng = Mo / kTcCols;
+    int gb, ge;  // this unit's column groups [gb, ge)
+    tc_unit_groups(unit, ng, &gb, &ge);
     float2* gbuf = reinterpret_cast<float2*>(sm + h * kTcGbufBytes);
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
     unsigned char* blo = bhi + kTcBBytes;
@@ -348,8 +354,8 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
                      (P.tmaps ? ((P.tmap_mask[R.out_buf >> 6] >> (R.out_buf & 63)) & 1ull) != 0 : R.out_buf == 0);
     if (P.tmaps && tma) tensormap_acquire(map);
     void* outb = P.outs[R.out_buf];
-    int g = h;
-    if (g < ng) {
+    int g = gb + h;
+    if (g < ge) {
         build_b_kp<true>(kp16, tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
@@ -363,8 +369,8 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
     const int amax = (n + Mo - 1) / Mo;  // stripes a that hold output samples
     // the halves run the same per-group sequence; starting half 1 a little later
     // keeps their DFT (issue-bound) and staging/store (SMEM-bound) phases apart
-    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
-    while (g < ng) {
+    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S, next_unit);
+    while (g < ge) {
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
         tc_fence_after();
@@ -388,7 +394,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators drained; the G buffer is free
         const int gn = g + 2;
-        if (gn < ng) build_b_kp<true>(kp16, tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
+        if (gn < ge) build_b_kp<true>(kp16, tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
 #pragma unroll
         for (int tt = 0; tt < 4; tt++) {
             const int k2 = lane + 32 * (8 * qd + tb + tt);
@@ -397,7 +403,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         }
         fence_proxy_async_smem();
         half_bar(h);  // G tiles and the next B in SMEM
-        if (lane == 0 && gn < ng) {
+        if (lane == 0 && gn < ge) {
             tc_fence_after();
             issue_group_kp<true>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
@@ -494,7 +500,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
                                            const float2* __restrict__ twhi, const float2* __restrict__ t2,
                                            uint32_t tmem, uint32_t mbar_h, uint32_t& phase, uint32_t mbar2_h,
                                            uint32_t& phase2, float* s_red, int* next_idx, RowDesc* next_R,
-                                           SigDesc* next_S, bool kp16) {
+                                           SigDesc* next_S, int* next_unit, int unit, bool kp16) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -516,6 +522,8 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const float fin = inv * (float)((kp16 ? 16 : 8) * 1024);
 
     const int ng = Mo / kTcCols;
+    int gb, ge;  // this unit's column groups [gb, ge)
+    tc_unit_groups(unit, ng, &gb, &ge);
     unsigned char* abuf = sm + h * kTcGbufBytes;        // DFT-stage A operand, 32 KB
     unsigned char* stage = abuf + kTcGbufBytes / 2;     // output staging, 32 KB
     unsigned char* bhi = sm + kTcOffB + h * 2 * kTcBBytes;
@@ -529,8 +537,8 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
                      (P.tmaps ? ((P.tmap_mask[R.out_buf >> 6] >> (R.out_buf & 63)) & 1ull) != 0 : R.out_buf == 0);
     if (P.tmaps && tma) tensormap_acquire(map);
     void* outb = P.outs[R.out_buf];
-    int g = h;
-    if (g < ng) {
+    int g = gb + h;
+    if (g < ge) {
         build_b_kp<false>(kp16, tg, g, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
         fence_proxy_async_smem();
         half_bar(h);
@@ -551,8 +559,8 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
     const int my_c = lane & 7;
     unsigned char* my_stage = stage + stage16_off(my_a1, my_c);
     const uint32_t dsrc = dcol + lane_base + 64u * (uint32_t)(wl >> 2);
-    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S);
-    while (g < ng) {
+    if (h == 1 && wl == 7 && lane == 0) tc_claim_next(P, next_idx, next_R, next_S, next_unit);
+    while (g < ge) {
         mbar_wait(mbar_h, phase, P.err);
         phase ^= 1u;
         tc_fence_after();
@@ -588,7 +596,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             mma_commit(mbar2_h);
         }
         const int gn = g + 2;
-        if (gn < ng) {
+        if (gn < ge) {
             build_b_kp<false>(kp16, tg, gn, ht, M, Nm, R.L, twlo, twhi, bhi, blo, D);
             fence_proxy_async_smem();
         }
@@ -637,7 +645,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
         tc_fence_before();
         if (tma && lane == 0 && wl >= 4) bulk_wait_read_all();
         half_bar(h);  // accumulators free for the next group; staging free
-        if (lane == 0 && gn < ng) {
+        if (lane == 0 && gn < ge) {
             tc_fence_after();
             issue_group_kp<false>(kp16, wl, tmem, dcol, bhi_a, blo_a);
             mma_commit(mbar_h);
@@ -694,6 +702,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __shared__ __align__(8) unsigned long long s_mbar2[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_idx[2];
+    __shared__ int s_unit[2];
     __shared__ int s_log2N;
     __shared__ RowDesc s_R[2];
     __shared__ SigDesc s_S[2];
@@ -746,7 +755,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int i = (int)atomicAdd(P.counter, 1u);
         s_idx[0] = i;
         if (i < P.n_list) {
-            s_R[0] = P.rows[P.row_list[i]];
+            s_unit[0] = P.row_list[i];
+            s_R[0] = P.rows[s_unit[0] & kUnitRowMask];
             s_S[0] = P.sigs[s_R[0].sig];
         }
     }
@@ -768,10 +778,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const float2* twhi = M <= kTcTwhiSmem ? twhi_s : S.tw + kP2;
         if constexpr (OT == OUT_BF16 || OT == OUT_F16) {
             row_tc_dft<OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, mbar2_h, phase2, s_red,
-                                &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1], R.kp > 8);
+                                &s_idx[sl ^ 1], &s_R[sl ^ 1], &s_S[sl ^ 1], &s_unit[sl ^ 1], s_unit[sl], R.kp > 8);
         } else {
             row_tc<OT, DEC>(P, &omap, R, S, sm, twlo, twhi, t2, tmem, mbar_h, phase, s_red, &s_idx[sl ^ 1],
-                            &s_R[sl ^ 1], &s_S[sl ^ 1], R.kp > 8);
+                            &s_R[sl ^ 1], &s_S[sl ^ 1], &s_unit[sl ^ 1], s_unit[sl], R.kp > 8);
         }
         tc_fence_before();
         __syncthreads();
