@@ -47,6 +47,7 @@ CASES = [
     (1, 2.0, LOGSCALES, 1000, 1.0, 100.0, 5, 1, True),
     (2, 2.0, LOGSCALES, 1000, 1.0, 100.0, 5, 1, True),
     (3, 2.0, LINFREQS, 1000, 1.0, 100.0, 5, 1, False),
+    (5, 2.0, LINFREQS, 1000, 1.0, 100.0, 5, 1, True),
     (17, 1.0, LOGSCALES, 1000, 10.0, 400.0, 9, 1, True),
     (100, 2.0, LOGSCALES, 1000, 5.0, 450.0, 20, 8, True),
     (511, 0.5, LINSCALES, 1000, 5.0, 450.0, 30, 3, True),
@@ -56,6 +57,7 @@ CASES = [
     (1024, 2.0, LOGSCALES, 1000, 2.0, 490.0, 64, 8, True),
     (1500, 0.5, LOGSCALES, 1000, 2.0, 490.0, 50, 1, False),
     (4096, 4.0, LINSCALES, 1000, 2.0, 490.0, 50, 2, True),
+    (6000, 2.0, LOGSCALES, 1000, 2.0, 490.0, 40, 1, True),
     (10000, 2.0, LINFREQS, 1000, 1.0, 101.0, 300, 1, True),
     (16384, 2.0, LOGSCALES, 1000, 2.0, 200.0, 128, 8, True),
     (16385, 2.0, LOGSCALES, 1000, 2.0, 200.0, 40, 8, True),
@@ -78,7 +80,7 @@ def test_cwt_vs_fp64_oracle(fcwt, oracle, case):
     assert rel_l2(exact, ref) < TOL
 
 
-@pytest.mark.parametrize("n", [1000, 4096, 30000])
+@pytest.mark.parametrize("n", [1000, 4096, 8000, 30000])
 def test_ccwt_complex_input(fcwt, oracle, n):
     rng = np.random.default_rng(11)
     x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
