@@ -659,6 +659,18 @@ def form_grad(steps: int, warmup: int, stream, check: bool = True) -> dict:
 
     ms_adj = _timed(adj, steps, warmup, stream)
     del y_keep, g_in
+    # the same loss through the power layer: |W|^2 from the row kernels' power
+    # epilogue, backward = recomputed W times 2 dL/dP into the same adjoint
+    layer_p = LearnableMorletCWT(freqs, 1000.0, sigma=2.0, power=True)
+
+    def step_power():
+        x.grad = None
+        layer_p.zero_grad()
+        P = layer_p(x)
+        loss = ((P - target) ** 2).mean()
+        loss.backward()
+
+    ms_p = _timed(step_power, steps, warmup, stream)
     points = B * F * n
     res = {"metric": "scalogram points/s (forward + backward)", "value": points / (ms / 1e3),
            "unit": "points/s", "ms_per_step": ms,
@@ -667,7 +679,10 @@ def form_grad(steps: int, warmup: int, stream, check: bool = True) -> dict:
                       "batch": B, "n": n, "fn": F},
            "forward_ms": ms_f, "adjoint_ms": ms_adj,
            "note": "step = forward transform + loss + hand-written adjoint (signal, sigma, frequencies); "
-                   "adjoint_ms = the backward of a kept forward alone"}
+                   "adjoint_ms = the backward of a kept forward alone",
+           "power_layer": {"value": points / (ms_p / 1e3), "ms_per_step": ms_p, "speedup": ms / ms_p,
+                           "what": "the same loss on LearnableMorletCWT(power=True): |W|^2 written by the "
+                                   "row kernels, backward recomputes W"}}
     if check:
         from oracle.grad_ref import power_mse, ref_forward
 
@@ -690,7 +705,16 @@ def form_grad(steps: int, warmup: int, stream, check: bool = True) -> dict:
                                    "sigma": abs(float(layer.sigma.grad) - float(sr.grad)) / abs(float(sr.grad)),
                                    "freqs_max": float(torch.max(torch.abs(layer.freqs.grad.cuda() - fr.grad))
                                                       / torch.max(torch.abs(fr.grad)))}
-        del yr, Lr, xr, y
+        step_power()
+        torch.cuda.synchronize()
+        with torch.no_grad():
+            P = layer_p(x).detach()
+        res["power_layer"]["rel_l2_vs_fp64"] = rel(P.double(), (yr.detach().abs() ** 2))
+        res["power_layer"]["grad_rel_vs_fp64"] = {
+            "signal": rel(x.grad.double(), xr.grad),
+            "sigma": abs(float(layer_p.sigma.grad) - float(sr.grad)) / abs(float(sr.grad)),
+            "freqs_max": float(torch.max(torch.abs(layer_p.freqs.grad.cuda() - fr.grad)) / torch.max(torch.abs(fr.grad)))}
+        del yr, Lr, xr, y, P
     return res
 
 

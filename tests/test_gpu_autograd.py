@@ -106,3 +106,71 @@ def test_learnable_module_trains():
     # moving the centre frequencies toward 40 Hz increases the energy
     assert float(layer.freqs.grad[0]) < 0 < float(layer.freqs.grad[1])
     assert e0 > 0 and layer.sigma.grad is not None and torch.isfinite(layer.sigma.grad)
+
+
+@pytest.mark.parametrize("n,F,norm", [(1500, 5, True), (20000, 9, True), (5000, 7, False)])
+def test_power_layer_forward_and_gradients(n, F, norm):
+    """morlet_power_cwt: |y|^2 from the power epilogue and its gradients
+    (recomputed y, dL/dy = 2 y dL/dP into the adjoint) against float64 torch
+    autograd of |ref_forward|^2 and central differences in sigma."""
+    import torch
+
+    from fcwt_b200.autograd import morlet_power_cwt
+
+    rng = np.random.default_rng(n + 7)
+    B, fs = 2, 1000.0
+    t = np.arange(n) / fs
+    x0 = np.stack([np.sin(2 * np.pi * (10 + 30 * t) * t) + 0.1 * rng.standard_normal(n) for _ in range(B)])
+    f0 = np.geomspace(5.0, 150.0, F)
+    sig0 = 2.0
+    target = torch.from_numpy(rng.uniform(0, 0.05, (B, F, n)))
+    if not norm:
+        target = target * (1 << int(math.ceil(math.log2(n)))) ** 2
+
+    x = torch.tensor(x0, dtype=torch.float32, device="cuda", requires_grad=True)
+    sigma = torch.tensor(sig0, dtype=torch.float64, requires_grad=True)
+    freqs = torch.tensor(f0, dtype=torch.float64, requires_grad=True)
+    P = morlet_power_cwt(x, sigma, freqs, fs, norm)
+    assert P.dtype == torch.float32 and P.shape == (B, F, n)
+    L = ((P.double().cpu() - target) ** 2).mean()
+    L.backward()
+
+    xr = torch.tensor(x0.astype(np.float32).astype(np.float64), requires_grad=True)
+    sr = torch.tensor(sig0, dtype=torch.float64, requires_grad=True)
+    fr = torch.tensor(f0, dtype=torch.float64, requires_grad=True)
+    Pr = ref_forward(xr, sr, fr, fs, norm).abs() ** 2
+    Lr = ((Pr - target) ** 2).mean()
+    Lr.backward()
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    assert rel(P.detach().cpu().double(), Pr.detach()) < 2e-5
+    assert rel(x.grad.cpu().double(), xr.grad) < 1e-4
+    assert abs(float(sigma.grad) - float(sr.grad)) <= 1e-4 * abs(float(sr.grad)) + 1e-12
+    assert float(torch.max(torch.abs(freqs.grad - fr.grad)) / torch.max(torch.abs(fr.grad))) < 1e-4
+
+    def L_at(sv):
+        with torch.no_grad():
+            p = ref_forward(xr.detach(), torch.tensor(sv, dtype=torch.float64), fr.detach(), fs, norm).abs() ** 2
+            return float(((p - target) ** 2).mean())
+    h = 1e-6
+    fd = (L_at(sig0 + h) - L_at(sig0 - h)) / (2 * h)
+    assert abs(float(sigma.grad) - fd) <= 1e-4 * abs(fd) + 1e-10
+
+
+def test_power_layer_module():
+    import torch
+
+    from fcwt_b200.autograd import LearnableMorletCWT
+
+    n, fs = 4096, 1000.0
+    t = np.arange(n) / fs
+    x = torch.tensor(np.sin(2 * np.pi * 40 * t), dtype=torch.float32, device="cuda").reshape(1, n)
+    lp = LearnableMorletCWT([30.0, 55.0], fs, sigma=2.0, power=True)
+    lc = LearnableMorletCWT([30.0, 55.0], fs, sigma=2.0)
+    P = lp(x)
+    y = lc(x)
+    assert torch.allclose(P, y.abs() ** 2, rtol=1e-5, atol=1e-7 * float(P.max()))
+    (-P.mean()).backward()
+    assert float(lp.freqs.grad[0]) < 0 < float(lp.freqs.grad[1])
