@@ -13,7 +13,7 @@ from .api import (DOG, FCWT, FCWT_LINFREQS, FCWT_LINSCALES, FCWT_LOGSCALES, Batc
 
 __all__ = ["Morlet", "Paul", "DOG", "Scales", "FCWT", "Wavelet", "FCWT_LINSCALES", "FCWT_LOGSCALES", "FCWT_LINFREQS", "cwt",
            "cwt_device", "Plan", "BatchPlan", "synchronize", "row_truncation", "mother_host", "FcwtError",
-           "morlet_cwt", "LearnableMorletCWT"]
+           "morlet_cwt", "morlet_power_cwt", "LearnableMorletCWT"]
 
 
 def __getattr__(name):
@@ -22,7 +22,7 @@ def __getattr__(name):
 
         return StreamingCWT
     # the differentiable operator needs torch; import it on first use
-    if name in ("morlet_cwt", "LearnableMorletCWT", "MorletCWTFunction"):
+    if name in ("morlet_cwt", "morlet_power_cwt", "LearnableMorletCWT", "MorletCWTFunction", "MorletPowerFunction"):
         from . import autograd
 
         return getattr(autograd, name)
