@@ -171,6 +171,6 @@ def test_power_layer_module():
     lc = LearnableMorletCWT([30.0, 55.0], fs, sigma=2.0)
     P = lp(x)
     y = lc(x)
-    assert torch.allclose(P, y.abs() ** 2, rtol=1e-5, atol=1e-7 * float(P.max()))
+    assert torch.allclose(P.detach(), y.detach().abs() ** 2, rtol=1e-5, atol=1e-7 * float(P.detach().max()))
     (-P.mean()).backward()
     assert float(lp.freqs.grad[0]) < 0 < float(lp.freqs.grad[1])
