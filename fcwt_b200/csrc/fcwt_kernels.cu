@@ -164,16 +164,23 @@ __device__ __forceinline__ void phase1_chunk(const SigDesc& S, const RowDesc& R,
         float2* __restrict__ dst = gdst + k2;
         // post-twiddle w_N^{base + d u}: exact every 8 outputs, running
         // product in between
+        // (output address and exponent advance by a step, which keeps the
+        // 32-output case from holding all addresses in registers)
         const float2 wd = tw_n(twlo, twhi, d);
         float2 w = make_float2(1.0f, 0.0f);
+        float2* p = dst + (size_t)v * kP2;
+        const size_t pstep = (size_t)Rr * kP2;
+        unsigned eu = base;
 #pragma unroll
         for (int u = 0; u < K; u++) {
-            w = (u & 7) ? cmul(w, wd) : tw_n(twlo, twhi, (base + (unsigned)u * d) & Nm);
+            w = (u & 7) ? cmul(w, wd) : tw_n(twlo, twhi, eu & Nm);
+            eu += d;
             const float2 g = cmul(z[u], w);
             if constexpr (TO_GLOBAL)
-                __stcg(dst + (size_t)(v + Rr * u) * kP2, g);
+                __stcg(p, g);
             else
-                dst[(v + Rr * u) * kP2] = g;
+                *p = g;
+            p += pstep;
         }
     }
     __syncthreads();
