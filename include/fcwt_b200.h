@@ -248,10 +248,10 @@ int fcwt_load_optimization_plan(fcwt_context* ctx, int n, int threads, const cha
  * legacy default stream). The call makes no host-to-device copies: its
  * descriptors reach the device as kernel parameters, so it does not wait for
  * earlier work in the stream (host-side planning still uses the C++ heap).
- * The first call on a device resolves the array's address and configures the
- * kernels for that device: make it before any stream capture. That address is
- * kept for the life of the process: do not call cudaDeviceReset while the
- * library is in use. All calls share the array: calls whose GPU work overlaps
+ * The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and configures the kernels for that device
+ * (cudaFuncSetAttribute). That address is kept for the life of the process:
+ * do not call cudaDeviceReset while the library is in use. All calls share the array: calls whose GPU work overlaps
  * race; serialize them on one stream. With status != NULL the call waits for
  * its work and stores the device error word there (0 = ok); with status ==
  * NULL it neither waits nor reads that word, so a device-side error is not
