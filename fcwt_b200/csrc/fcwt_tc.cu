@@ -698,7 +698,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float2* twlo = reinterpret_cast<float2*>(sm + kTcOffTwlo);
     float2* t2 = reinterpret_cast<float2*>(sm + kTcOffT2);
     float2* twhi_s = reinterpret_cast<float2*>(sm + kTcOffTwhi);
-    __shared__ __align__(8) unsigned long long s_mbar[2];
+    // Completion of the phase-1 MMAs of half h. The 16-bit outputs use one
+    // barrier per tile half p (tiles 4 p .. 4 p + 3, issued and drained by warps
+    // 4 p .. 4 p + 3 of the half), so that a warp waits only for the tiles it
+    // drains: 4% faster for BF16; complex64 measured 0.2% slower with it and
+    // keeps one barrier per half.
+    constexpr bool kSplitP1 = OT == OUT_BF16 || OT == OUT_F16;
+    __shared__ __align__(8) unsigned long long s_mbar[4];
     __shared__ __align__(8) unsigned long long s_mbar2[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_idx[2];
@@ -731,8 +737,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         fence_proxy_async_smem();
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_u32(&s_mbar[1])));
+        for (int k = 0; k < 4; k++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_mbar[k])), "r"(kSplitP1 ? 4 : 8));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar2[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar2[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -747,7 +753,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const uint32_t mbar_h = smem_u32(&s_mbar[h]);
+    const uint32_t mbar_h = smem_u32(&s_mbar[kSplitP1 ? 2 * h + ((warp & 7) >> 2) : h]);
     const uint32_t mbar2_h = smem_u32(&s_mbar2[h]);
     uint32_t phase = 0, phase2 = 0;
 
