@@ -315,8 +315,11 @@ __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __re
             w = cmul(w, stp);
         }
         fft_reg<32, +1>(x);
-#pragma unroll
-        for (int u1 = 1; u1 < 32; u1++) x[u1] = cmul(x[u1], twhi[((unsigned)(j * u1 * Rr)) & Mm]);
+    };
+    // twiddle w_K^{j u1} = w_M^{j u1 R} of task t, applied as the FFT32 outputs are stored
+    auto post_tw = [&](int t, int u1) -> float2 {
+        const int j = (t >> 3) % K2;
+        return twhi[((unsigned)(j * u1 * Rr)) & Mm];
     };
     for (int v0 = 0; v0 < Rr; v0 += VBn) {
         const int VB = min(VBn, Rr - v0);
@@ -327,14 +330,16 @@ __device__ void phase1_big(const SigDesc& S, const RowDesc& R, const float* __re
             float2 x[32];
             fft32_task(tid, v0, x);
             __syncthreads();
+            Y[tid] = x[0];
 #pragma unroll
-            for (int u1 = 0; u1 < 32; u1++) Y[u1 * TP + tid] = x[u1];
+            for (int u1 = 1; u1 < 32; u1++) Y[u1 * TP + tid] = cmul(x[u1], post_tw(tid, u1));
         } else {
             for (int t = tid; t < T; t += kThreads) {
                 float2 x[32];
                 fft32_task(t, v0, x);
+                Y[t] = x[0];
 #pragma unroll
-                for (int u1 = 0; u1 < 32; u1++) Y[u1 * TP + t] = x[u1];
+                for (int u1 = 1; u1 < 32; u1++) Y[u1 * TP + t] = cmul(x[u1], post_tw(t, u1));
             }
         }
         __syncthreads();
