@@ -108,7 +108,24 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// tcgen05.wait::ld with the destination registers of the loads it completes
+// as operands, so that no read of them can be placed before the wait.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+    asm volatile(""
+                 : "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
@@ -380,7 +397,7 @@ __device__ __forceinline__ void row_tc(const TcParams& P, const CUtensorMap* oma
         for (int tt = 0; tt < 4; tt++) {
             uint32_t r[16];
             tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
-            tmem_wait_ld();
+            tmem_wait_ld(r);
             const int k2 = lane + 32 * (8 * qd + tb + tt);
             float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], inv));
             const float2 stp = DEC ? tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm) : twlo[k2];
@@ -571,7 +588,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             for (int tt = 0; tt < 4; tt++) {
                 uint32_t r[16];
                 tmem_ld16(dcol + lane_base + 16u * (tb + tt), r);
-                tmem_wait_ld();
+                tmem_wait_ld(r);
                 const int k2 = lane + 32 * (8 * qd + tb + tt);
                 float2 w = cmul(tw_n(twlo, twhi, ((unsigned)(k2 - lane) * (unsigned)(D * c0)) & Nm), cscale(tg[lane], s1));
                 const float2 stp = DEC ? tw_n(twlo, twhi, ((unsigned)k2 * (unsigned)D) & Nm) : twlo[k2];
@@ -609,7 +626,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             uint32_t r[32];
             tmem_ld16(dsrc + 32u * q2, *reinterpret_cast<uint32_t(*)[16]>(r));
             tmem_ld16(dsrc + 32u * q2 + 16u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
-            tmem_wait_ld();
+            tmem_wait_ld(r);
 #pragma unroll
             for (int i = 0; i < 16; i++) {
                 const int a1 = 16 * q2 + i;
@@ -636,7 +653,7 @@ __device__ __forceinline__ void row_tc_dft(const TcParams& P, const CUtensorMap*
             uint32_t r[32];
             tmem_ld16(dsrc + 32u * q2, *reinterpret_cast<uint32_t(*)[16]>(r));
             tmem_ld16(dsrc + 32u * q2 + 16u, *reinterpret_cast<uint32_t(*)[16]>(r + 16));
-            tmem_wait_ld();
+            tmem_wait_ld(r);
 #pragma unroll
             for (int i = 0; i < 16; i++)
                 yv[16 * q2 + i] = pack16<OT>(
