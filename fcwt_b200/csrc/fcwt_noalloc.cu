@@ -80,7 +80,7 @@ constexpr size_t kNoAllocScratchBytes = align256(kOffScratch + sizeof(float2) * 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // ---- descriptor delivery by kernel parameters (at most 32764 bytes each)
-constexpr int kRowsPerCopy = 232;    // 232 x 112-byte RowDesc
+constexpr int kRowsPerCopy = 232;    // RowDesc per launch (232 x 120 B)
 constexpr int kFloatsPerCopy = 7680; // 30 KB of stale-bin table entries
 
 struct RowCopy {
