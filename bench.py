@@ -218,7 +218,7 @@ def run_reference_arm(args, rank: int) -> None:
     line = {
         "impl": "reference", "metric": "scalogram points/s", "value": v, "unit": "points/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-        "higher_is_better": True, "scaling": "weak" if args.gpus <= 1 else "strong", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": plain_config(),
         "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": "reference",
                          "sample": f"full workload, {args.steps} timed calls of FCWT::cwt (FFTW 3.3.10 + OpenMP, "
@@ -376,7 +376,7 @@ def main():
     achieved = algo / (eng_avg / 1e3) / 1e9
     line = {
         "metric": "scalogram points/s", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": plain_config(fn, args.out),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
