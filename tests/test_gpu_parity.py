@@ -294,3 +294,30 @@ def test_compat_align_shift_reproduces_reference_rows(fcwt, oracle, reference, n
     fcwt.FCWT(fcwt.Morlet(2.0), 2, False, norm).cwt(x, sc, clean)
     ref64 = oracle.cwt_fp64(x, sc, 2.0, 2, norm)
     assert rel_l2(clean, ref64) < 1e-5
+
+
+def test_split_work_units_equal_whole_rows(fcwt, oracle):
+    """The tensor-core queue splits the last rows of a launch into 2, 4 or 8
+    column-group parts. A 7-row shard of the 100k x 3000 grid runs every row
+    as parts; inside the full 3000-row plan rows 0-6 and 1500-1506 are whole
+    units, and its last 74 rows are halves. Every split computes each column
+    group the same way, so the rows are bit-equal."""
+    import torch
+
+    n = 100000
+    x = torch.from_numpy(np.random.default_rng(11).standard_normal(n).astype(np.float32)).cuda()
+    sc = oracle.scales(LINFREQS, 1000, 1.0, 101.0, 3000)
+    full = torch.empty((3000, n), dtype=torch.complex64, device="cuda")
+    p = fcwt.Plan(n, sc, fb=2.0, threads=8, norm=True)
+    assert p.stats()["tensor_core_rows"] == 3000
+    p.execute(x, full)
+    p.close()
+    for rb, re_ in [(0, 7), (1500, 1507), (2993, 3000)]:
+        ps = fcwt.Plan(n, sc, fb=2.0, threads=8, norm=True, rows=(rb, re_))
+        part = torch.full((re_ - rb, n), float("nan"), dtype=torch.complex64, device="cuda")
+        ps.execute(x, part)
+        ps.close()
+        torch.cuda.synchronize()
+        assert torch.equal(part, full[rb:re_]), (rb, re_)
+    del full
+    torch.cuda.empty_cache()
